@@ -1,0 +1,350 @@
+#!/usr/bin/env python
+"""Benchmark of the fused BGK_PCM time step on B200.
+
+One "step" is one time step of the cavity workload (every node of the grid
+advances f, g and phi once, STEP_7/main.f90:60-69).  Default workload: the
+2048x2048 cavity at Ra=1e6, FP64 (cavity2048_ra1e6), i.e. the configuration
+the headline metric is quoted on; its populations (604 MB) are larger than
+L2, so consecutive steps never hit a warm cache.
+
+  value     GLUPS = Nx*Ny*steps / device time / 1e9, summed over ranks
+  e2e       the same metric through the public C ABI with host buffers: the
+            initial state uploaded from pinned host memory, the steps with the
+            reference's diagnostic cadence (sums + probe every 1000 steps), and
+            the final fields downloaded, all inside the timed region
+  roofline  algorithmic bytes per launch of the fused kernel / its average
+            duration, against the measured HBM copy bandwidth
+  cpu_baseline  the CPU oracle (C restatement of STEP_7, OpenMP over all host
+            threads) on a bounded number of steps of the same workload
+
+`--impl reference` times that CPU implementation alone as the reference arm.
+Multi-GPU (torchrun, N ranks): every rank runs its own replica of the
+workload (weak scaling); the step has no cross-rank data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "GLUPS & HBM GB/s: FP32-store vs FP64 at ≤1e-4 err; adjoint/forward cost"
+BYTES_PER_NODE = {"f64": 304, "f32": 152, "f16": 80}
+FALLBACK_HBM = 6650.0
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    REASONS = {
+        0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap",
+        0x8: "hw_slowdown", 0x10: "sync_boost", 0x20: "sw_thermal_slowdown",
+        0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting",
+    }
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 4:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+                bits = int(parts[3], 16) if parts[3].startswith("0x") else int(parts[3])
+            except ValueError:
+                continue
+            for b, n in self.REASONS.items():
+                if bits & b:
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_oracle_rate(params, budget_s: float = 15.0, max_steps: int = 400):
+    """GLUPS of the CPU oracle (all host threads) on whole steps of `params`."""
+    from oracle import pyoracle
+    threads = os.cpu_count() or 1
+    o = pyoracle.Oracle(params, threads=threads)
+    o.initialization()
+    t0 = time.perf_counter()
+    o.step(2)
+    dt = (time.perf_counter() - t0) / 2
+    n = int(max(2, min(max_steps, budget_s / max(dt, 1e-9))))
+    t0 = time.perf_counter()
+    o.step(n)
+    t = time.perf_counter() - t0
+    o.close()
+    glups = params["Nx"] * params["Ny"] * n / t / 1e9
+    return glups, n, threads
+
+
+def load_traffic(kernel_key: str):
+    """Per-launch DRAM bytes of a kernel from the committed ncu summary."""
+    f = ROOT / "profiles" / "ncu_traffic.json"
+    if not f.exists():
+        return None
+    d = json.loads(f.read_text())
+    return d.get(kernel_key, {}).get("traffic_bytes_per_launch")
+
+
+def time_steps(solver, steps: int, torch):
+    stream = torch.cuda.ExternalStream(solver.stream)
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    solver.step(steps)
+    end.record(stream)
+    end.synchronize()
+    return start.elapsed_time(end)
+
+
+def e2e_run(params, precision, steps, device, torch):
+    """Public-API run with host buffers: upload, steps + diag cadence, download."""
+    import numpy as np
+
+    from bgk_pcm_b200 import Solver
+    Nx, Ny = params["Nx"], params["Ny"]
+    shape = (Ny + 2, Nx + 2)
+    names = [f"f{k}" for k in range(9)] + [f"g{k}" for k in range(9)] + ["rho", "T", "u", "v", "phi"]
+    src = Solver(params, precision=precision, device=device)
+    src.initialization()
+    host_in = {}
+    for n in names:
+        t = torch.empty(shape, dtype=torch.float64, pin_memory=True)
+        a = t.numpy()
+        a[:] = src.field(n)
+        host_in[n] = (t, a)
+    src.close()
+    outs = {n: torch.empty(shape, dtype=torch.float64, pin_memory=True) for n in ("rho", "T", "u", "v", "phi")}
+    s = Solver(params, precision=precision, device=device)
+    stream = torch.cuda.ExternalStream(s.stream)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    h2d = 0
+    for n in names:
+        s.upload(n, host_in[n][1])
+        h2d += host_in[n][1].nbytes
+    d2h = 0
+    done = 0
+    while done < steps:
+        chunk = min(1000, steps - done)
+        s.step(chunk)
+        done += chunk
+        sums = s.sums()
+        probe = s.region("T", Nx // 2, Ny // 2, 1, 1)
+        d2h += sums.nbytes + probe.nbytes
+    for n, t in outs.items():
+        a = s.field(n, out=t.numpy())
+        d2h += a.nbytes
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    s.close()
+    return ms, h2d, d2h
+
+
+def run_reference(args, params, wl):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    glups, n, threads = cpu_oracle_rate(params, budget_s=min(60.0, 5.0 + 0.5 * args.steps), max_steps=args.steps)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": glups, "unit": "GLUPS", "n_gpus": args.gpus,
+        "steps": n, "warmup": 0, "ms_per_step": params["Nx"] * params["Ny"] / glups / 1e6,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (the reference's initial condition on the generated input.dat)",
+        "config": {"workload": args.workload, "Nx": params["Nx"], "Ny": params["Ny"], "Ra": wl["Ra"],
+                   "Pr": wl["Pr"], "Ste": wl["Ste"], "precision": "f64"},
+        "cpu_baseline": {"value": glups, "unit": "GLUPS", "cores": threads, "kind": "port",
+                         "sample": f"{n} whole steps of the {params['Nx']}x{params['Ny']} grid; C restatement of "
+                                   "STEP_7 (OpenMP, bit-identical to serial); the Fortran reference cannot be "
+                                   "compiled in this image"},
+        "e2e": {"value": glups, "unit": "GLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10000)
+    ap.add_argument("--warmup", type=int, default=100)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cavity2048_ra1e6")
+    ap.add_argument("--precision", default="f64", choices=["f64", "f32", "f16"])
+    ap.add_argument("--forms", default="f64fma", help="extra forms timed beside the headline (comma list)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    from bgk_pcm_b200 import inputs
+    wl = inputs.WORKLOADS[args.workload]
+    params = inputs.workload_params(**wl)
+
+    if args.impl == "reference":
+        run_reference(args, params, wl)
+        return
+
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from bgk_pcm_b200 import Solver, build
+    build.build()
+
+    Nx, Ny = params["Nx"], params["Ny"]
+    nodes = Nx * Ny
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def run_form(precision, fma, steps, warmup, sample_clocks=False):
+        s = Solver(params, precision=precision, fma=fma, device=local)
+        s.initialization()
+        s.step(warmup)
+        s.sync()
+        clocks = None
+        sampler = ClockSampler(local) if sample_clocks else None
+        barrier()
+        torch.cuda.synchronize()
+        if sampler:
+            sampler.start()
+            time.sleep(0.3)
+        ms = time_steps(s, steps, torch)
+        torch.cuda.synchronize()
+        if sampler:
+            clocks = sampler.stop()
+        barrier()
+        s.close()
+        return ms, clocks
+
+    ms, clocks = run_form(args.precision, False, args.steps, args.warmup, sample_clocks=True)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = nodes * args.steps * world / (ms / 1e3) / 1e9
+    hbm, hbm_kind = peaks()
+    bpn = BYTES_PER_NODE[args.precision]
+    achieved = bpn * nodes / (ms / 1e3 / args.steps) / 1e9
+    kernel_key = f"fused_{args.precision}_{args.workload}"
+    traffic = load_traffic(kernel_key)
+
+    forms = {}
+    for form in [f for f in args.forms.split(",") if f]:
+        prec, fma = ("f64", True) if form == "f64fma" else (form, False)
+        try:
+            fms, _ = run_form(prec, fma, max(args.steps // 4, 100), args.warmup)
+        except Exception as exc:  # a form that is not available is reported, not fatal
+            forms[form] = {"error": str(exc)}
+            continue
+        g = nodes * max(args.steps // 4, 100) / (fms / 1e3) / 1e9
+        b = BYTES_PER_NODE[prec]
+        forms[form] = {"glups": g, "hbm_gbs": g * b, "frac_of_measured_hbm": g * b / hbm,
+                       "bytes_per_node": b}
+
+    e2e = None
+    if not args.no_e2e:
+        e_ms, h2d, d2h = e2e_run(params, args.precision, args.steps, local, torch)
+        if dist:
+            t = torch.tensor([e_ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_ms = float(t.item())
+        e2e = {"value": nodes * args.steps * world / (e_ms / 1e3) / 1e9, "unit": "GLUPS",
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+               "what": "initial state (23 reference-layout fields) uploaded from pinned host memory, the steps "
+                       "with field sums + probe read back every 1000 steps, final rho/T/u/v/phi downloaded"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        glups, n, threads = cpu_oracle_rate(params)
+        cpu = {"value": glups, "unit": "GLUPS", "cores": threads, "kind": "port",
+               "sample": f"{n} whole steps of the {Nx}x{Ny} grid, C restatement of STEP_7 with OpenMP "
+                         "(bit-identical to serial)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GLUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": args.precision,
+            "data": "synthetic: the reference's initial condition on the generated input.dat",
+            "config": {"workload": args.workload, "Nx": Nx, "Ny": Ny, "Ra": wl["Ra"], "Pr": wl["Pr"],
+                       "Ste": wl["Ste"], "precision": args.precision, "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2 (A/B populations %.0f MB > 126 MB)"
+                             % (2 * 18 * {"f64": 8, "f32": 4, "f16": 2}[args.precision] * nodes / 1e6)},
+            "hbm_gbs": value / world * bpn,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": traffic, "peak_kind": hbm_kind,
+                         "bytes_per_node": bpn},
+            "forms": forms,
+            "clocks": clocks,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "gpu_launches": args.steps + 1,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,155 @@
+/*
+ * fused_f64.cuh -- the fused FP64 time-step kernel.  Included by
+ * kernels_f64.cu (built with --fmad=false: bit-for-bit the reference's
+ * operation order) and by kernels_fast.cu (built with multiply-add
+ * contraction: the FMA variant, same source).  Must be included inside an
+ * anonymous namespace within namespace bgk, after select_tanh.
+ */
+#ifndef BGK_FUSED_F64_CUH
+#define BGK_FUSED_F64_CUH
+
+/* ------------------------------------------------------------ fused step */
+
+constexpr int FUSED_BX = 128;
+
+/* One thread owns one column x of a strip of H rows and marches up it.  The
+ * 3x3 phi stencil is kept as per-cell selector terms (aplus/aminus) of a
+ * sliding 3-row window, so each phi value is loaded and squared once per row
+ * instead of nine times.  Populations are pulled from the neighbours
+ * (STEP_7/streaming.f90:5-27) with the no-slip boundary folded in:
+ *  f: a pull from outside the domain takes the opposite population of the
+ *     same node (bounce-back), except f6 at (Nx,1) and f7 at (Nx,Ny), which
+ *     read the never-written corner halos (kept in corner[0..1]);
+ *  g: rows 0/Ny+1 are copies of rows 1/Ny (clamp y), column 0 is the west
+ *     value, column Nx+1 is w_k*T(Nx,y)*poly_k (east, previous moments). */
+template <int TANH, bool MOM>
+__global__ void __launch_bounds__(FUSED_BX)
+fused_f64_kernel(StepPtrs<double> s, Consts c, const double *__restrict__ corner, int H)
+{
+    const int Nx = c.Nx, Ny = c.Ny;
+    const int x = blockIdx.x * FUSED_BX + threadIdx.x;
+    if (x >= Nx) return;
+    const int y0 = blockIdx.y * H;
+    const int y1 = min(y0 + H, Ny);
+    const long long pl = s.plane;
+    const int P = s.P;
+    const bool W = (x == 0), E = (x == Nx - 1);
+    const double *__restrict__ F = s.fin;
+    const double *__restrict__ G = s.gin;
+    const double *__restrict__ PH = s.phin;
+
+    double ap[3][3], am[3][3], pc[3];
+    auto load_row = [&](int r, int slot) {
+        const int rc = r < 0 ? 0 : (r >= Ny ? Ny - 1 : r);
+        const double *row = PH + (long long)rc * P;
+        const double pL = *(W ? (s.phiW + rc) : (row + x - 1));
+        const double pM = row[x];
+        const double pR = *(E ? (s.phiE + rc) : (row + x + 1));
+        ap[slot][0] = aplus(pL); ap[slot][1] = aplus(pM); ap[slot][2] = aplus(pR);
+        am[slot][0] = aminus(pL); am[slot][1] = aminus(pM); am[slot][2] = aminus(pR);
+        pc[slot] = pM;
+    };
+    load_row(y0 - 1, 0);
+    load_row(y0, 1);
+
+    for (int y = y0; y < y1; y++) {
+        load_row(y + 1, 2);
+        const bool S = (y == 0), N = (y == Ny - 1);
+        const long long cc = (long long)y * P + x;
+
+        /* streaming (pull) with bounce-back */
+        double f[9], g[9];
+        f[0] = F[cc];
+        f[1] = *(W ? F + 3 * pl + cc : F + 1 * pl + cc - 1);
+        f[2] = *(S ? F + 4 * pl + cc : F + 2 * pl + cc - P);
+        f[3] = *(E ? F + 1 * pl + cc : F + 3 * pl + cc + 1);
+        f[4] = *(N ? F + 2 * pl + cc : F + 4 * pl + cc + P);
+        f[5] = *((W || S) ? F + 7 * pl + cc : F + 5 * pl + cc - P - 1);
+        f[6] = *((E || S) ? F + 8 * pl + cc : F + 6 * pl + cc - P + 1);
+        f[7] = *((E || N) ? F + 5 * pl + cc : F + 7 * pl + cc + P + 1);
+        f[8] = *((W || N) ? F + 6 * pl + cc : F + 8 * pl + cc + P - 1);
+        if (E && S) f[6] = corner[0];
+        if (E && N) f[7] = corner[1];
+
+        /* streaming of g with the BC_g halo values */
+        const int ym = S ? y : y - 1, yp = N ? y : y + 1;
+        const long long cm = (long long)ym * P + x, cp = (long long)yp * P + x;
+        g[0] = G[cc];
+        g[1] = *(W ? s.gW + y : G + 1 * pl + cc - 1);
+        g[2] = G[2 * pl + cm];
+        g[4] = G[4 * pl + cp];
+        g[5] = *(W ? s.gW + Ny + ym : G + 5 * pl + cm - 1);
+        g[8] = *(W ? s.gW + 2 * Ny + yp : G + 8 * pl + cp - 1);
+        if (E) {
+            g[3] = c.w[3] * s.tcin[y] * s.pE[y];
+            g[6] = c.w[6] * s.tcin[ym] * s.pE[Ny + ym];
+            g[7] = c.w[7] * s.tcin[yp] * s.pE[2 * Ny + yp];
+        } else {
+            g[3] = G[3 * pl + cc + 1];
+            g[6] = G[6 * pl + cm + 1];
+            g[7] = G[7 * pl + cp + 1];
+        }
+
+        /* momentsPre */
+        const double rho = sum9(f);
+        double T = sum9(g);
+        const double irho = 1.0 / rho;
+        double u = irho * xmom(f);
+        double v = irho * ymom(f);
+        const double T2 = T, u2 = u, v2 = v;
+
+        /* phase_field */
+        const double th = select_tanh(((T - c.T_crit) - c.T_act) / c.T_width, TANH);
+        const double kp = ap[1][1] + ap[1][2] + ap[2][1] + ap[1][0] + ap[0][1]
+                        + ap[2][2] + ap[2][0] + ap[0][0] + ap[0][2];
+        const double km = am[1][1] + am[1][2] + am[2][1] + am[1][0] + am[0][1]
+                        + am[2][2] + am[2][0] + am[0][0] + am[0][2];
+        const double p0 = pc[1];
+        const double phn = phi_update(c, kp, km, th, p0);
+
+        /* forces */
+        apply_forces(c, phn, p0, rho, T, u, v);
+
+        /* collision */
+        double Pq[9], eq[9], out[9];
+        eq_poly(u, v, Pq);
+#pragma unroll
+        for (int k = 0; k < 9; k++) eq[k] = c.w[k] * rho * Pq[k];
+        regularize_relax(c, f, eq, c.omega_f, out);
+#pragma unroll
+        for (int k = 0; k < 9; k++) { s.fout[k * pl + cc] = out[k]; f[k] = out[k]; }
+#pragma unroll
+        for (int k = 0; k < 9; k++) eq[k] = c.w[k] * T * Pq[k];
+        regularize_relax(c, g, eq, c.omega_g, out);
+#pragma unroll
+        for (int k = 0; k < 9; k++) s.gout[k * pl + cc] = out[k];
+        s.phout[cc] = phn;
+
+        /* moments (all nodes on output steps; column Nx every step) */
+        if (MOM || E) {
+            const double Tm = (sum9(out) + T2) * 0.5;
+            if (E) s.tcout[y] = Tm;
+            if (MOM) {
+                const double rm = sum9(f);
+                const double irm = 1.0 / rm;
+                const double tu = irm * xmom(f);
+                const double tv = irm * ymom(f);
+                const size_t q = (size_t)(x + 1) + (size_t)s.NX2 * (size_t)(y + 1);
+                s.mrho[q] = rm;
+                s.mT[q] = Tm;
+                s.mu[q] = (tu + u2) * 0.5;
+                s.mv[q] = (tv + v2) * 0.5;
+                s.mphi[q] = phn;
+            }
+        }
+
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            ap[0][k] = ap[1][k]; ap[1][k] = ap[2][k];
+            am[0][k] = am[1][k]; am[1][k] = am[2][k];
+        }
+        pc[0] = pc[1]; pc[1] = pc[2];
+    }
+}
+
+#endif

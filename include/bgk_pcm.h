@@ -1,0 +1,185 @@
+/*
+ * bgk_pcm.h -- C ABI of the B200 (sm_100a) implementation of the BGK_PCM
+ * time step: D2Q9 double-distribution thermal lattice Boltzmann (f = flow,
+ * g = temperature), regularized BGK collision, buoyancy + solid drag forcing
+ * and the kinetic phase-field update with latent-heat feedback.
+ *
+ * The reference (giacomofalcucci/BGK_PCM, STEP_7/) has no library interface:
+ * its boundary is a set of argument-less Fortran subroutines that mutate the
+ * module `shared` (STEP_7/shared.f90:1-104), called in a fixed order from
+ * STEP_7/main.f90:60-69.  Each entry point below replaces one of them (cited
+ * per function); bgk_step replaces the whole sequence with one fused kernel
+ * per time step.  The only C interop precedent in the reference is
+ * STEP_7/get_mem.c:23 bound by STEP_7/get_mem_mod.f90:7, and these functions
+ * follow the same style: plain C types, bind(c)-friendly.
+ *
+ * Conventions
+ *  - Every function returns BGK_OK (0) or a negative BGK_ERR_* code and never
+ *    exits, aborts or traps; bgk_last_error() describes the last failure of
+ *    the calling thread.
+ *  - Host arrays use the reference layout: a field is (0:Nx+1, 0:Ny+1)
+ *    column-major (x fastest), halos included, with a leading dimension
+ *    ld >= Nx+2 (ld = Nx+2 for a Fortran array declared like the reference's).
+ *  - A context owns its device buffers and one CUDA stream; it is used by one
+ *    host thread at a time.  Calls that return data synchronise the stream;
+ *    bgk_step and the stage entry points only enqueue work.
+ *  - There is no CPU fallback: a context can only be created on a CUDA device
+ *    of compute capability 10.0 (B200), and every step runs on it.
+ */
+#ifndef BGK_PCM_H
+#define BGK_PCM_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+#define BGK_OK               0
+#define BGK_ERR_ARG         -1  /* invalid argument                              */
+#define BGK_ERR_UNSUPPORTED -2  /* valid input the chosen path does not implement */
+#define BGK_ERR_CUDA        -3  /* CUDA runtime or launch failure                 */
+#define BGK_ERR_OOM         -4  /* device or host allocation failed               */
+#define BGK_ERR_STATE       -5  /* call not allowed in the current state          */
+#define BGK_ERR_IO          -6  /* file could not be read or written              */
+#define BGK_ERR_NONFINITE   -7  /* a reduction found NaN or Inf                    */
+
+/* ------------------------------------------------------------- parameters */
+/* The 21 input.dat values in file order (STEP_7/setup.f90:7-31). */
+typedef struct bgk_params {
+    int iter, noutput, dump, Nx, Ny;
+    double Re, rho0, rho1, tau_f, tau_g, T0, T_in_sol, grav, eps,
+           stefan_number, T_width, length;
+    int westBC, eastBC, northBC, southBC;
+} bgk_params;
+
+/* Storage/arithmetic form of the populations. */
+#define BGK_PREC_F64   0  /* plain FP64 (the reference's mykind = dp)                  */
+#define BGK_PREC_F32   1  /* FP32 deviations f_i - w_i*rho0, g_i - w_i*T0, FP32 math    */
+#define BGK_PREC_F16   2  /* FP16 deviations with a per-field scale, FP32 math          */
+
+/* tanh used by the phase-field selector (STEP_7/phase_field.f90:20-21). */
+#define BGK_TANH_DEVICE   0  /* CUDA's tanh (production)                              */
+#define BGK_TANH_PORTABLE 1  /* bgk_portable_tanh.h: bit-identical CPU/GPU check mode */
+
+typedef struct bgk_options {
+    int precision;   /* BGK_PREC_*                                              */
+    int tanh_mode;   /* BGK_TANH_*                                              */
+    int fma;         /* FP64 only: 0 = the reference's exact operation order    */
+                     /* (no fused multiply-add); 1 = FMA-contracted variant      */
+    int device;      /* CUDA device ordinal, or -1 for the current device        */
+} bgk_options;
+
+/* ----------------------------------------------------------------- fields */
+/* Field ids for bgk_upload / bgk_download; the names are the reference's
+ * arrays (STEP_7/shared.f90:36-79). */
+#define BGK_FIELD_F0        0   /* f0..f8   =  0..8  */
+#define BGK_FIELD_G0        9   /* g0..g8   =  9..17 */
+#define BGK_FIELD_RHO      18
+#define BGK_FIELD_T        19
+#define BGK_FIELD_U        20
+#define BGK_FIELD_V        21
+#define BGK_FIELD_PHI      22
+#define BGK_FIELD_PHI_PREC 23
+#define BGK_FIELD_RHO2     24
+#define BGK_FIELD_T2       25
+#define BGK_FIELD_U2       26
+#define BGK_FIELD_V2       27
+#define BGK_FIELD_FP0      28   /* fp0..fp8 = 28..36 */
+#define BGK_FIELD_GP0      37   /* gp0..gp8 = 37..45 */
+#define BGK_NFIELDS        46
+
+typedef struct bgk_ctx bgk_ctx;
+
+/* Thread-local description of the last failure ("" if none). */
+const char *bgk_last_error(void);
+
+/* Parse input.dat (list-directed "label value" records, d/D exponents and
+ * trailing comments accepted).  Replaces STEP_7/setup.f90:5-32. */
+int bgk_read_input(const char *path, bgk_params *out);
+
+/* Allocate device state and derive the constants (weights, omega_f, omega_g,
+ * kvisc, alpha).  Replaces STEP_7/setup.f90:34-115.  opt may be NULL
+ * (FP64, device tanh, exact order, current device).  The fused step supports
+ * the no-slip code 4 on all four walls, the only code any shipped input uses
+ * (UTIL/input.dat.0-3); the staged entry points also run BC_f codes
+ * 0/1/2/3/5/6 (FP64 only). */
+int bgk_create(const bgk_params *p, const bgk_options *opt, bgk_ctx **out);
+int bgk_destroy(bgk_ctx *ctx);
+
+/* Fill every field with the reference's initial condition: liquid strip
+ * i <= Nx/40 at (T0, rho1, phi=+1), solid elsewhere at (T_in_sol, rho0,
+ * phi=-1), equilibrium populations; sets it = 0.  Replaces
+ * STEP_7/initialization.f90:5-152. */
+int bgk_initialize(bgk_ctx *ctx);
+
+/* nsteps fused time steps, each equivalent to STEP_7/main.f90:60-69
+ * (BC_f, BC_g, streaming, momentsPre, phase_field, forces, collision,
+ * moments); advances it by nsteps.  Afterwards rho, T, u, v, phi (with
+ * halos) are as the reference leaves them after `moments`. */
+int bgk_step(bgk_ctx *ctx, int nsteps);
+
+/* One reference subroutine each, unfused, on the complete reference state
+ * (FP64 contexts only).  Calling them in the order of STEP_7/main.f90:60-69
+ * gives results bit-identical to bgk_step(ctx, 1).  bgk_moments increments it.
+ * A context may switch between staged and fused stepping at step
+ * boundaries (after bgk_moments). */
+int bgk_bc_f(bgk_ctx *ctx);          /* STEP_7/BC_f.f90:1-207         */
+int bgk_bc_g(bgk_ctx *ctx);          /* STEP_7/BC_g.f90:1-71          */
+int bgk_streaming(bgk_ctx *ctx);     /* STEP_7/streaming.f90:1-33     */
+int bgk_moments_pre(bgk_ctx *ctx);   /* STEP_7/momentsPre.f90:1-71    */
+int bgk_phase_field(bgk_ctx *ctx);   /* STEP_7/phase_field.f90:1-63   */
+int bgk_forces(bgk_ctx *ctx);        /* STEP_7/forces.f90:1-43        */
+int bgk_collision(bgk_ctx *ctx);     /* STEP_7/collision.f90:1-158    */
+int bgk_moments(bgk_ctx *ctx);       /* STEP_7/moments.f90:1-74       */
+
+/* Copy one field between the host (reference layout, leading dimension ld)
+ * and the device.  After bgk_step the fields f, g, rho, T, u, v, phi and
+ * phi_prec can be downloaded; the momentsPre copies (rho2, T2, u2, v2) and
+ * the streamed populations (fp, gp) exist only in the staged state.
+ * Uploading f, g, rho, T, u, v or phi replaces that part of the state, the
+ * way STEP_7/dump_in.f90:9-18 overwrites the module arrays. */
+int bgk_upload(bgk_ctx *ctx, int field, const double *host, int ld);
+int bgk_download(bgk_ctx *ctx, int field, double *host, int ld);
+
+/* Copy the rectangle i0..i0+ni-1, j0..j0+nj-1 (reference indices, halos
+ * allowed) of a field into host[a + ld*b].  Used for the probe, the x/y
+ * profiles and the wall-gradient columns of the diagnostics
+ * (STEP_7/probe.f90, prof_x.f90, prof_y.f90, diag.f90:63-76) without copying
+ * the whole field. */
+int bgk_download_region(bgk_ctx *ctx, int field, int i0, int j0, int ni, int nj,
+                        double *host, int ld);
+
+/* Interior reductions in FP64 for field_check/diag
+ * (STEP_7/field_check.f90:9-17, STEP_7/diag.f90:82-91):
+ * out[0] = sum rho, out[1] = sum T, out[2] = sum phi, out[3] = #(phi > 0).
+ * Returns BGK_ERR_NONFINITE (with out filled) if a sum is NaN or Inf. */
+int bgk_field_sums(bgk_ctx *ctx, double out[4]);
+
+/* Time-step counter `it` (STEP_7/main.f90:54). */
+int bgk_get_it(const bgk_ctx *ctx, int *it);
+int bgk_set_it(bgk_ctx *ctx, int it);
+
+/* Hot-wall temperature per row: tin[j-1] is Tin for row j = 1..Ny
+ * (generalises the scalar Tin of STEP_7/BC_g.f90:13-16; tin = NULL restores
+ * the scalar Tin = T0 of STEP_7/initialization.f90:9). */
+int bgk_set_tin(bgk_ctx *ctx, const double *tin, int ny);
+
+/* Wait for all work queued on the context's stream. */
+int bgk_sync(bgk_ctx *ctx);
+
+/* The context's CUDA stream (a cudaStream_t), so a caller can order its own
+ * work or timing events with the library's kernels.  No reference
+ * counterpart (the reference has no device streams). */
+int bgk_get_stream(bgk_ctx *ctx, void **stream);
+
+/* Complete binary snapshot (populations, phi, frozen boundary values, it)
+ * -- unlike the reference's text dump (STEP_7/dump_out.f90:5-18), which omits
+ * phi and phi_prec.  A snapshot restores into a context of the same size and
+ * precision. */
+int bgk_save(bgk_ctx *ctx, const char *path);
+int bgk_load(bgk_ctx *ctx, const char *path);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BGK_PCM_H */

@@ -1,0 +1,16 @@
+/* Command-line driver for the CPU oracle: runs the STEP_7 program in a
+ * directory holding input.dat (TEST INFRASTRUCTURE ONLY).
+ * usage: orc_main <dir> [threads] [tanh_mode] */
+#include "step7.h"
+#include <stdio.h>
+#include <stdlib.h>
+
+int main(int argc, char **argv)
+{
+    if (argc < 2) { fprintf(stderr, "usage: %s <dir> [threads] [tanh_mode]\n", argv[0]); return 2; }
+    int nt = argc > 2 ? atoi(argv[2]) : 0;
+    int tm = argc > 3 ? atoi(argv[3]) : 0;
+    int rc = orc_main(argv[1], nt, tm);
+    if (rc) fprintf(stderr, "orc_main failed: %d\n", rc);
+    return rc ? 1 : 0;
+}
