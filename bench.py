@@ -290,7 +290,7 @@ def main():
     traffic = load_traffic(kernel_key)
 
     forms = {}
-    for form in [f for f in args.forms.split(",") if f]:
+    for form in [f for f in args.forms.split(",") if f and f != "none"]:
         prec, fma = ("f64", True) if form == "f64fma" else (form, False)
         try:
             fms, _ = run_form(prec, fma, max(args.steps // 4, 100), args.warmup)

@@ -15,6 +15,11 @@
  *  - forces: `beta` is never declared and forces.f90 has no `implicit none`,
  *    so it is an implicit default REAL (4 bytes): its value is rounded to
  *    float and promoted back (STEP_7/forces.f90:13).
+ *  - collision: the temporaries are declared as ft00..ft08 / gt00..gt08
+ *    (STEP_7/collision.f90:11-12) but the code assigns ft0..ft8 / gt0..gt8
+ *    (collision.f90:84-120), which are therefore implicit REAL(4) as well:
+ *    each regularized population is rounded to float before the relaxation
+ *    f = ft - omega*(ft - feq) is evaluated in double.
  *  - BC_f with code 4 never writes f6(Nx+1,0) nor f7(Nx+1,Ny+1); streaming
  *    reads them, so they keep their initial equilibrium values.
  *  - BC_g's north/south copies run after its west/east fills, so the corner
@@ -626,7 +631,8 @@ void orc_collision(orc_state *s)
     for (int j = 1; j <= Ny; j++)
         for (int i = 1; i <= Nx; i++) {
             size_t q = IX(i, j);
-            double fe[9], ge[9], d[9], e[9], ft[9], gt[9];
+            double fe[9], ge[9], d[9], e[9];
+            float ft[9], gt[9]; /* implicit REAL(4): ft0..ft8, gt0..gt8 are undeclared */
             feq9(s->w, RHO[q], UU[q], VV[q], fe);
             feq9(s->w, TT[q], UU[q], VV[q], ge);
             for (int k = 0; k < 9; k++) { d[k] = FP(k)[q] - fe[k]; e[k] = GP(k)[q] - ge[k]; }
@@ -659,8 +665,8 @@ void orc_collision(orc_state *s)
             gt[7] = ge[7] + C[7] * (q1 * txx + q1 * tyy + 2.0 * txy);
             gt[8] = ge[8] + C[8] * (q1 * txx + q1 * tyy - 2.0 * txy);
             for (int k = 0; k < 9; k++) {
-                F(k)[q] = ft[k] - omf * (ft[k] - fe[k]);
-                G(k)[q] = gt[k] - omg * (gt[k] - ge[k]);
+                F(k)[q] = (double)ft[k] - omf * ((double)ft[k] - fe[k]);
+                G(k)[q] = (double)gt[k] - omg * ((double)gt[k] - ge[k]);
             }
         }
 }
