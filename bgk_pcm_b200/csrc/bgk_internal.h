@@ -123,6 +123,11 @@ struct bgk_ctx {
     double *corner;        /* f6(Nx+1,0), f7(Nx+1,Ny+1) (never written by BC_f) */
     int red_n;
     double *pinned;        /* small pinned host buffer                      */
+
+    /* launch shape of the fused kernels: strip height (0 = automatic) and
+     * L2 prefetch distance in rows (0 = off); BGK_STRIP_H / BGK_PREFETCH_ROWS
+     * override the defaults at bgk_create */
+    int tune_H, tune_pf;
 };
 
 namespace bgk {

@@ -386,6 +386,10 @@ int bgk_create(const bgk_params *pp, const bgk_options *opt, bgk_ctx **out)
     c->it = 0;
     c->cur = 0;
     c->bc_dirty = true;
+    c->tune_H = 0;
+    c->tune_pf = 2;
+    if (const char *v = getenv("BGK_STRIP_H")) c->tune_H = atoi(v);
+    if (const char *v = getenv("BGK_PREFETCH_ROWS")) c->tune_pf = atoi(v);
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { delete c; return cuda_fail(e, "cudaStreamCreate"); }
 

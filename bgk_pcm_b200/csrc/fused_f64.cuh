@@ -12,6 +12,36 @@
 
 constexpr int FUSED_BX = 128;
 
+/* Bulk prefetch of one row segment into L2 (sm_90+ bulk-copy unit): a hint
+ * that keeps DRAM requests in flight without registers or shared memory.
+ * ptr must be 16-byte aligned, bytes a multiple of 16. */
+__device__ __forceinline__ void prefetch_l2(const void *ptr, unsigned bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(ptr), "r"(bytes) : "memory");
+}
+
+/* Threads 0..18 of a strip block prefetch source row r of the nine f
+ * planes, the nine g planes and the phi plane for columns x0..x0+127. */
+template <typename T, typename TP>
+__device__ __forceinline__ void prefetch_row(const T *F, const T *G, const TP *PH, long long pl, int P, int x0,
+                                             int ncols, int r, int Ny)
+{
+    const int t = threadIdx.x;
+    if (t >= 19 || r >= Ny) return;
+    const long long off = (long long)r * P + x0;
+    const void *ptr;
+    unsigned bytes;
+    if (t < 18) {
+        ptr = (t < 9 ? F + t * pl : G + (t - 9) * pl) + off;
+        bytes = (unsigned)(ncols * sizeof(T));
+    } else {
+        ptr = PH + off;
+        bytes = (unsigned)(ncols * sizeof(TP));
+    }
+    bytes = (bytes + 15u) & ~15u;
+    prefetch_l2(ptr, bytes);
+}
+
 /* One thread owns one column x of a strip of H rows and marches up it.  The
  * 3x3 phi stencil is kept as per-cell selector terms (aplus/aminus) of a
  * sliding 3-row window, so each phi value is loaded and squared once per row
@@ -23,8 +53,8 @@ constexpr int FUSED_BX = 128;
  *  g: rows 0/Ny+1 are copies of rows 1/Ny (clamp y), column 0 is the west
  *     value, column Nx+1 is w_k*T(Nx,y)*poly_k (east, previous moments). */
 template <int TANH, bool MOM>
-__global__ void __launch_bounds__(FUSED_BX)
-fused_f64_kernel(StepPtrs<double> s, Consts c, const double *__restrict__ corner, int H)
+__global__ void __launch_bounds__(FUSED_BX, 4)
+fused_f64_kernel(StepPtrs<double> s, Consts c, const double *__restrict__ corner, int H, int pf)
 {
     const int Nx = c.Nx, Ny = c.Ny;
     const int x = blockIdx.x * FUSED_BX + threadIdx.x;
@@ -52,7 +82,9 @@ fused_f64_kernel(StepPtrs<double> s, Consts c, const double *__restrict__ corner
     load_row(y0 - 1, 0);
     load_row(y0, 1);
 
+    const int x0 = blockIdx.x * FUSED_BX, ncols = min(FUSED_BX, Nx - x0);
     for (int y = y0; y < y1; y++) {
+        if (pf > 0) prefetch_row(F, G, PH, pl, P, x0, ncols, y + pf, Ny);
         load_row(y + 1, 2);
         const bool S = (y == 0), N = (y == Ny - 1);
         const long long cc = (long long)y * P + x;

@@ -593,6 +593,7 @@ cudaError_t launch_macro_halos(bgk_ctx *c)
 static int strip_height(const bgk_ctx *c)
 {
     /* enough blocks to fill 148 SMs several times over, but tall strips */
+    if (c->tune_H > 0) return c->tune_H;
     const int bx = (c->Nx + FUSED_BX - 1) / FUSED_BX;
     int H = 16;
     while (H > 2 && (long long)bx * ((c->Ny + H - 1) / H) < 148LL * 8) H /= 2;
@@ -615,11 +616,11 @@ cudaError_t launch_fused_f64(bgk_ctx *c, bool moments)
     const double *corner = corner_ptr(c);
     const bool portable = c->opt.tanh_mode == BGK_TANH_PORTABLE;
     if (portable) {
-        if (moments) fused_f64_kernel<BGK_TANH_PORTABLE, true><<<grd, FUSED_BX, 0, c->stream>>>(s, c->c, corner, H);
-        else fused_f64_kernel<BGK_TANH_PORTABLE, false><<<grd, FUSED_BX, 0, c->stream>>>(s, c->c, corner, H);
+        if (moments) fused_f64_kernel<BGK_TANH_PORTABLE, true><<<grd, FUSED_BX, 0, c->stream>>>(s, c->c, corner, H, c->tune_pf);
+        else fused_f64_kernel<BGK_TANH_PORTABLE, false><<<grd, FUSED_BX, 0, c->stream>>>(s, c->c, corner, H, c->tune_pf);
     } else {
-        if (moments) fused_f64_kernel<BGK_TANH_DEVICE, true><<<grd, FUSED_BX, 0, c->stream>>>(s, c->c, corner, H);
-        else fused_f64_kernel<BGK_TANH_DEVICE, false><<<grd, FUSED_BX, 0, c->stream>>>(s, c->c, corner, H);
+        if (moments) fused_f64_kernel<BGK_TANH_DEVICE, true><<<grd, FUSED_BX, 0, c->stream>>>(s, c->c, corner, H, c->tune_pf);
+        else fused_f64_kernel<BGK_TANH_DEVICE, false><<<grd, FUSED_BX, 0, c->stream>>>(s, c->c, corner, H, c->tune_pf);
     }
     return cudaGetLastError();
 }

@@ -1,0 +1,78 @@
+"""Reduced-precision forms (FP32 and FP16 deviation storage) against the FP64
+path on the same cavity.  Errors are normalised as the precision targets are
+stated: T by the temperature span dT = T0 - T_in_sol, phi by its range 2,
+u and v by max |u| of the FP64 run.  Bound for the FP32 form: 1e-4 on T and
+phi (max relative); the FP16 form is reported with a loose sanity bound."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import small_params
+
+pytestmark = pytest.mark.gpu
+
+
+def run(precision, p, steps):
+    from bgk_pcm_b200 import Solver
+    s = Solver(p, precision=precision)
+    s.initialization()
+    s.step(steps)
+    out = {n: s.field(n)[1:-1, 1:-1] for n in ("rho", "T", "u", "v", "phi")}
+    s.close()
+    return out
+
+
+def errors(a, b, p):
+    dT = p["T0"] - p["T_in_sol"]
+    umax = max(np.abs(a["u"]).max(), np.abs(a["v"]).max(), 1e-30)
+    return {
+        "T": np.abs(a["T"] - b["T"]).max() / dT,
+        "phi": np.abs(a["phi"] - b["phi"]).max() / 2.0,
+        "u": np.abs(a["u"] - b["u"]).max() / umax,
+        "v": np.abs(a["v"] - b["v"]).max() / umax,
+        "rho": np.abs(a["rho"] - b["rho"]).max(),
+    }
+
+
+def test_fp32_form_within_1e4(lib):
+    p = small_params(128, 128)
+    ref = run("f64", p, 3000)
+    lo = run("f32", p, 3000)
+    e = errors(ref, lo, p)
+    assert e["T"] <= 1e-4 and e["phi"] <= 1e-4, e
+    assert e["u"] <= 1e-2 and e["v"] <= 1e-2, e
+
+
+def test_fp16_form_runs(lib):
+    p = small_params(96, 64)
+    ref = run("f64", p, 1000)
+    lo = run("f16", p, 1000)
+    for v in lo.values():
+        assert np.isfinite(v).all()
+    e = errors(ref, lo, p)
+    assert e["T"] < 5e-2 and e["phi"] < 5e-2, e
+
+
+@pytest.mark.parametrize("precision", ["f32", "f16"])
+def test_lowp_upload_download(lib, precision):
+    """Deviation storage round-trips the reference layout within its precision."""
+    from bgk_pcm_b200 import Solver
+    p = small_params(40, 30)
+    a = Solver(p); a.initialization(); a.step(5)
+    b = Solver(p, precision=precision); b.initialization()
+    for n in [f"f{k}" for k in range(9)] + [f"g{k}" for k in range(9)] + ["rho", "T", "u", "v", "phi"]:
+        b.upload(n, a.field(n))
+    tol = {"f32": 1e-6, "f16": 2e-3}[precision]
+    for n in ("f1", "g5"):
+        np.testing.assert_allclose(b.field(n)[1:-1, 1:-1], a.field(n)[1:-1, 1:-1], rtol=tol, atol=tol)
+    a.step(3); b.step(3)
+    np.testing.assert_allclose(b.field("T")[1:-1, 1:-1], a.field("T")[1:-1, 1:-1], rtol=0, atol=20 * tol)
+
+
+def test_lowp_staged_unsupported(lib):
+    from bgk_pcm_b200 import BGKError, Solver
+    s = Solver(small_params(16, 16), precision="f32")
+    s.initialization()
+    with pytest.raises(BGKError, match="UNSUPPORTED"):
+        s.BC_f()

@@ -27,7 +27,10 @@ def test_threads_bit_identical(oracle_mod):
 
 def test_collision_conserves_node_moments(oracle_mod):
     """Regularized BGK keeps sum f = rho and sum g = T per node (the
-    non-equilibrium part carries no mass): collision.f90:94-111."""
+    non-equilibrium part carries no mass): collision.f90:94-111.  The
+    reference keeps its regularized populations ft0..ft8 / gt0..gt8 in
+    implicit REAL(4) variables, so the identity holds to float precision
+    (|1-omega| * sum|ft| * 2**-24), not to double precision."""
     o = oracle_mod.Oracle(small_params(20, 16))
     o.initialization()
     o.step(25)
@@ -37,8 +40,10 @@ def test_collision_conserves_node_moments(oracle_mod):
     o.stage("collision")
     sf = sum(o.field(f"f{k}") for k in range(9))
     sg = sum(o.field(f"g{k}") for k in range(9))
-    np.testing.assert_allclose(sf[1:-1, 1:-1], rho[1:-1, 1:-1], rtol=1e-13)
-    np.testing.assert_allclose(sg[1:-1, 1:-1], T[1:-1, 1:-1], rtol=1e-13)
+    np.testing.assert_allclose(sf[1:-1, 1:-1], rho[1:-1, 1:-1], rtol=2e-7)
+    np.testing.assert_allclose(sg[1:-1, 1:-1], T[1:-1, 1:-1], rtol=2e-7)
+    # and it is not exact in double: the float rounding is really there
+    assert np.abs(sg[1:-1, 1:-1] - T[1:-1, 1:-1]).max() > 0
 
 
 def test_equilibrium_solid_is_stationary(oracle_mod):
