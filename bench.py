@@ -37,7 +37,9 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "GLUPS & HBM GB/s: FP32-store vs FP64 at ≤1e-4 err; adjoint/forward cost"
-BYTES_PER_NODE = {"f64": 304, "f32": 152, "f16": 80}
+# algorithmic bytes per node and step: 18 populations + phi, read once and
+# written once (FP64; FP32/FP16 deviations with phi kept in FP64)
+BYTES_PER_NODE = {"f64": 304, "f32": 160, "f16": 88}
 FALLBACK_HBM = 6650.0
 
 

@@ -74,7 +74,7 @@ class Params(ctypes.Structure):
 
 class Options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("tanh_mode", ctypes.c_int), ("fma", ctypes.c_int),
-                ("device", ctypes.c_int)]
+                ("device", ctypes.c_int), ("smooth", ctypes.c_int)]
 
 
 class BGKError(RuntimeError):

@@ -97,6 +97,7 @@ struct bgk_ctx {
     int P;                 /* compact pitch                                 */
     long long plane;       /* Ny*P                                          */
     size_t esz;            /* bytes per stored population element           */
+    size_t phisz;          /* bytes per stored phi element (4 or 8)          */
     int it;
 
     /* fused state */

@@ -43,6 +43,7 @@ BGK_HD void eq_poly(double u, double v, double *P)
 
 /* Regularized BGK for one distribution (STEP_7/collision.f90:42-150):
  * in = streamed populations, eq = equilibria, out = post-collision. */
+template <bool REF32 = true>
 BGK_HD void regularize_relax(const Consts &c, const double *in, const double *eq,
                              double omega, double *out)
 {
@@ -65,16 +66,26 @@ BGK_HD void regularize_relax(const Consts &c, const double *in, const double *eq
     double s6 = sqq - tp;
     /* ft0..ft8 / gt0..gt8 are undeclared in collision.f90, hence implicit
      * REAL(4): the regularized population is rounded to float, then the
-     * relaxation is evaluated in double with it. */
-    double ft0 = (double)(float)(eq[0] + c.C[0] * s0);
-    double ft1 = (double)(float)(eq[1] + c.C[1] * s1);
-    double ft2 = (double)(float)(eq[2] + c.C[2] * s2);
-    double ft3 = (double)(float)(eq[3] + c.C[3] * s1);
-    double ft4 = (double)(float)(eq[4] + c.C[4] * s2);
-    double ft5 = (double)(float)(eq[5] + c.C[5] * s5);
-    double ft6 = (double)(float)(eq[6] + c.C[6] * s6);
-    double ft7 = (double)(float)(eq[7] + c.C[7] * s5);
-    double ft8 = (double)(float)(eq[8] + c.C[8] * s6);
+     * relaxation is evaluated in double with it (REF32; the smooth form
+     * keeps it in double). */
+    double ft0 = eq[0] + c.C[0] * s0;
+    if (REF32) ft0 = (double)(float)ft0;
+    double ft1 = eq[1] + c.C[1] * s1;
+    if (REF32) ft1 = (double)(float)ft1;
+    double ft2 = eq[2] + c.C[2] * s2;
+    if (REF32) ft2 = (double)(float)ft2;
+    double ft3 = eq[3] + c.C[3] * s1;
+    if (REF32) ft3 = (double)(float)ft3;
+    double ft4 = eq[4] + c.C[4] * s2;
+    if (REF32) ft4 = (double)(float)ft4;
+    double ft5 = eq[5] + c.C[5] * s5;
+    if (REF32) ft5 = (double)(float)ft5;
+    double ft6 = eq[6] + c.C[6] * s6;
+    if (REF32) ft6 = (double)(float)ft6;
+    double ft7 = eq[7] + c.C[7] * s5;
+    if (REF32) ft7 = (double)(float)ft7;
+    double ft8 = eq[8] + c.C[8] * s6;
+    if (REF32) ft8 = (double)(float)ft8;
     out[0] = ft0 - omega * (ft0 - eq[0]);
     out[1] = ft1 - omega * (ft1 - eq[1]);
     out[2] = ft2 - omega * (ft2 - eq[2]);

@@ -346,7 +346,7 @@ int bgk_create(const bgk_params *pp, const bgk_options *opt, bgk_ctx **out)
     *out = nullptr;
     int rc = check_params(*pp);
     if (rc) return rc;
-    bgk_options o{BGK_PREC_F64, BGK_TANH_DEVICE, 0, -1};
+    bgk_options o{BGK_PREC_F64, BGK_TANH_DEVICE, 0, -1, 0};
     if (opt) o = *opt;
     if (o.precision < BGK_PREC_F64 || o.precision > BGK_PREC_F16) return fail(BGK_ERR_ARG, "bad precision %d", o.precision);
     if (o.tanh_mode != BGK_TANH_DEVICE && o.tanh_mode != BGK_TANH_PORTABLE) return fail(BGK_ERR_ARG, "bad tanh_mode");
@@ -383,6 +383,12 @@ int bgk_create(const bgk_params *pp, const bgk_options *opt, bgk_ctx **out)
     c->P = (pp->Nx + 31) / 32 * 32;
     c->plane = (long long)c->P * pp->Ny;
     c->esz = o.precision == BGK_PREC_F64 ? 8 : (o.precision == BGK_PREC_F32 ? 4 : 2);
+    /* reduced-precision forms keep phi in FP64 unless BGK_LP_PHI32=1 */
+    c->phisz = 8;
+    if (o.precision != BGK_PREC_F64) {
+        const char *v = getenv("BGK_LP_PHI32");
+        if (v && atoi(v) == 1) c->phisz = 4;
+    }
     c->it = 0;
     c->cur = 0;
     c->bc_dirty = true;
@@ -395,7 +401,7 @@ int bgk_create(const bgk_params *pp, const bgk_options *opt, bgk_ctx **out)
 
     /* 9 planes per distribution plus one row of guard on each side */
     const size_t popbytes = (size_t)(9 * c->plane + 2 * c->P) * c->esz;
-    const size_t phibytes = (size_t)(c->plane + 2 * c->P) * (c->esz == 2 ? 4 : c->esz);
+    const size_t phibytes = (size_t)(c->plane + 2 * c->P) * c->phisz;
     for (int b = 0; b < 2; b++) {
         DA(c->fbuf[b], popbytes, "f populations");
         DA(c->gbuf[b], popbytes, "g populations");
@@ -673,7 +679,7 @@ int bgk_save(bgk_ctx *c, const char *path)
     const int hdr[8] = {c->Nx, c->Ny, c->opt.precision, c->it, c->P, c->tin_host ? 1 : 0, 0, 0};
     bool ok = fwrite(kMagic, 1, 8, fp) == 8 && fwrite(hdr, sizeof hdr, 1, fp) == 1;
     const size_t popbytes = (size_t)9 * c->plane * c->esz;
-    const size_t phibytes = (size_t)c->plane * (c->esz == 2 ? 4 : c->esz);
+    const size_t phibytes = (size_t)c->plane * c->phisz;
     std::vector<char> buf(std::max(popbytes, c->A * sizeof(double)));
     auto put = [&](const void *dev, size_t bytes) {
         if (!ok) return;
@@ -716,7 +722,7 @@ int bgk_load(bgk_ctx *c, const char *path)
                     hdr[2], c->Nx, c->Ny, c->opt.precision);
     }
     const size_t popbytes = (size_t)9 * c->plane * c->esz;
-    const size_t phibytes = (size_t)c->plane * (c->esz == 2 ? 4 : c->esz);
+    const size_t phibytes = (size_t)c->plane * c->phisz;
     std::vector<char> buf(std::max(popbytes, c->A * sizeof(double)));
     auto get = [&](void *dev, size_t bytes) {
         if (!ok) return;

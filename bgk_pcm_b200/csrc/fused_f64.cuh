@@ -52,7 +52,7 @@ __device__ __forceinline__ void prefetch_row(const T *F, const T *G, const TP *P
  *     read the never-written corner halos (kept in corner[0..1]);
  *  g: rows 0/Ny+1 are copies of rows 1/Ny (clamp y), column 0 is the west
  *     value, column Nx+1 is w_k*T(Nx,y)*poly_k (east, previous moments). */
-template <int TANH, bool MOM>
+template <int TANH, bool MOM, bool REF32>
 __global__ void __launch_bounds__(FUSED_BX, 4)
 fused_f64_kernel(StepPtrs<double> s, Consts c, const double *__restrict__ corner, int H, int pf)
 {
@@ -147,12 +147,12 @@ fused_f64_kernel(StepPtrs<double> s, Consts c, const double *__restrict__ corner
         eq_poly(u, v, Pq);
 #pragma unroll
         for (int k = 0; k < 9; k++) eq[k] = c.w[k] * rho * Pq[k];
-        regularize_relax(c, f, eq, c.omega_f, out);
+        regularize_relax<REF32>(c, f, eq, c.omega_f, out);
 #pragma unroll
         for (int k = 0; k < 9; k++) { s.fout[k * pl + cc] = out[k]; f[k] = out[k]; }
 #pragma unroll
         for (int k = 0; k < 9; k++) eq[k] = c.w[k] * T * Pq[k];
-        regularize_relax(c, g, eq, c.omega_g, out);
+        regularize_relax<REF32>(c, g, eq, c.omega_g, out);
 #pragma unroll
         for (int k = 0; k < 9; k++) s.gout[k * pl + cc] = out[k];
         s.phout[cc] = phn;
@@ -182,6 +182,23 @@ fused_f64_kernel(StepPtrs<double> s, Consts c, const double *__restrict__ corner
         }
         pc[0] = pc[1]; pc[1] = pc[2];
     }
+}
+
+/* Launch the fused kernel with the template arguments the context selects. */
+inline cudaError_t launch_fused_f64_variant(const bgk_ctx *c, dim3 grd, const StepPtrs<double> &s, int H, bool mom)
+{
+    const bool portable = c->opt.tanh_mode == BGK_TANH_PORTABLE;
+    const bool ref32 = !c->opt.smooth;
+#define BGK_LAUNCH(T, M, R) fused_f64_kernel<T, M, R><<<grd, FUSED_BX, 0, c->stream>>>(s, c->c, c->corner, H, c->tune_pf)
+    if (portable) {
+        if (mom) { if (ref32) BGK_LAUNCH(BGK_TANH_PORTABLE, true, true); else BGK_LAUNCH(BGK_TANH_PORTABLE, true, false); }
+        else { if (ref32) BGK_LAUNCH(BGK_TANH_PORTABLE, false, true); else BGK_LAUNCH(BGK_TANH_PORTABLE, false, false); }
+    } else {
+        if (mom) { if (ref32) BGK_LAUNCH(BGK_TANH_DEVICE, true, true); else BGK_LAUNCH(BGK_TANH_DEVICE, true, false); }
+        else { if (ref32) BGK_LAUNCH(BGK_TANH_DEVICE, false, true); else BGK_LAUNCH(BGK_TANH_DEVICE, false, false); }
+    }
+#undef BGK_LAUNCH
+    return cudaGetLastError();
 }
 
 #endif

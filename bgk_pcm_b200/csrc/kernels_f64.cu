@@ -398,6 +398,7 @@ __global__ void staged_forces(Staged s, Consts c)
 }
 
 /* STEP_7/collision.f90:14-152 */
+template <bool REF32>
 __global__ void staged_collision(Staged s, Consts c)
 {
     INTERIOR_IJ();
@@ -405,10 +406,10 @@ __global__ void staged_collision(Staged s, Consts c)
     const double rho = s.rho[q], T = s.T[q];
     eq_poly(s.u[q], s.v[q], Pq);
     for (int k = 0; k < 9; k++) { in[k] = s.fp[k][q]; eq[k] = c.w[k] * rho * Pq[k]; }
-    regularize_relax(c, in, eq, c.omega_f, out);
+    regularize_relax<REF32>(c, in, eq, c.omega_f, out);
     for (int k = 0; k < 9; k++) s.f[k][q] = out[k];
     for (int k = 0; k < 9; k++) { in[k] = s.gp[k][q]; eq[k] = c.w[k] * T * Pq[k]; }
-    regularize_relax(c, in, eq, c.omega_g, out);
+    regularize_relax<REF32>(c, in, eq, c.omega_g, out);
     for (int k = 0; k < 9; k++) s.g[k][q] = out[k];
 }
 
@@ -614,15 +615,8 @@ cudaError_t launch_fused_f64(bgk_ctx *c, bool moments)
     const int H = strip_height(c);
     dim3 grd((c->Nx + FUSED_BX - 1) / FUSED_BX, (c->Ny + H - 1) / H);
     const double *corner = corner_ptr(c);
-    const bool portable = c->opt.tanh_mode == BGK_TANH_PORTABLE;
-    if (portable) {
-        if (moments) fused_f64_kernel<BGK_TANH_PORTABLE, true><<<grd, FUSED_BX, 0, c->stream>>>(s, c->c, corner, H, c->tune_pf);
-        else fused_f64_kernel<BGK_TANH_PORTABLE, false><<<grd, FUSED_BX, 0, c->stream>>>(s, c->c, corner, H, c->tune_pf);
-    } else {
-        if (moments) fused_f64_kernel<BGK_TANH_DEVICE, true><<<grd, FUSED_BX, 0, c->stream>>>(s, c->c, corner, H, c->tune_pf);
-        else fused_f64_kernel<BGK_TANH_DEVICE, false><<<grd, FUSED_BX, 0, c->stream>>>(s, c->c, corner, H, c->tune_pf);
-    }
-    return cudaGetLastError();
+    (void)corner;
+    return launch_fused_f64_variant(c, grd, s, H, moments);
 }
 
 cudaError_t launch_staged(bgk_ctx *c, int stage)
@@ -643,7 +637,10 @@ cudaError_t launch_staged(bgk_ctx *c, int stage)
             staged_phase_field<BGK_TANH_DEVICE><<<grd, blk, 0, c->stream>>>(s, c->c);
         break;
     case 6: staged_forces<<<grd, blk, 0, c->stream>>>(s, c->c); break;
-    case 7: staged_collision<<<grd, blk, 0, c->stream>>>(s, c->c); break;
+    case 7:
+        if (c->opt.smooth) staged_collision<false><<<grd, blk, 0, c->stream>>>(s, c->c);
+        else staged_collision<true><<<grd, blk, 0, c->stream>>>(s, c->c);
+        break;
     case 8: staged_moments<<<grd, blk, 0, c->stream>>>(s, c->c); break;
     default: return cudaErrorInvalidValue;
     }

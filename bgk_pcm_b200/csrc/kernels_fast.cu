@@ -48,14 +48,7 @@ cudaError_t launch_fused_fast(bgk_ctx *c, bool moments)
     s.plane = c->plane; s.P = c->P; s.NX2 = c->NX2;
     const int H = strip_height(c);
     dim3 grd((c->Nx + FUSED_BX - 1) / FUSED_BX, (c->Ny + H - 1) / H);
-    if (c->opt.tanh_mode == BGK_TANH_PORTABLE) {
-        if (moments) fused_f64_kernel<BGK_TANH_PORTABLE, true><<<grd, FUSED_BX, 0, c->stream>>>(s, c->c, c->corner, H, c->tune_pf);
-        else fused_f64_kernel<BGK_TANH_PORTABLE, false><<<grd, FUSED_BX, 0, c->stream>>>(s, c->c, c->corner, H, c->tune_pf);
-    } else {
-        if (moments) fused_f64_kernel<BGK_TANH_DEVICE, true><<<grd, FUSED_BX, 0, c->stream>>>(s, c->c, c->corner, H, c->tune_pf);
-        else fused_f64_kernel<BGK_TANH_DEVICE, false><<<grd, FUSED_BX, 0, c->stream>>>(s, c->c, c->corner, H, c->tune_pf);
-    }
-    return cudaGetLastError();
+    return launch_fused_f64_variant(c, grd, s, H, moments);
 }
 
 namespace {
@@ -85,6 +78,7 @@ struct ConstsLP {
     float gb;                /* grav * beta                                  */
     float omega_f;
     double dts, T0d, rho0d;
+    double T0mTcrit_d, inv_T_width_d;
     double w_d[9];
 };
 
@@ -92,6 +86,10 @@ template <typename S> struct Codec;
 template <> struct Codec<float> {
     static __device__ __forceinline__ float ld(const float *p, float) { return __ldg(p); }
     static __device__ __forceinline__ void st(float *p, float v, float) { *p = v; }
+};
+template <> struct Codec<double> {
+    static __device__ __forceinline__ float ld(const double *p, float) { return (float)__ldg(p); }
+    static __device__ __forceinline__ void st(double *p, float v, float) { *p = (double)v; }
 };
 template <> struct Codec<__half> {
     static __device__ __forceinline__ float ld(const __half *p, float inv) { return __half2float(__ldg(p)) * inv; }
@@ -144,12 +142,12 @@ __device__ __forceinline__ void reg_relax_lp(const ConstsLP &c, const float *in,
     out[8] = eq[8] + cc[8] * s6;
 }
 
-template <typename S>
+template <typename S, typename PT>
 struct LpPtrs {
     const S *fin, *gin;
     S *fout, *gout;
-    const float *phin;
-    float *phout;
+    const PT *phin;
+    PT *phout;
     const double *tcin;
     double *tcout;
     const double *gW, *pE, *phiW, *phiE, *corner;
@@ -159,9 +157,22 @@ struct LpPtrs {
     float sf, sg, inv_sf, inv_sg;
 };
 
-template <typename S, int TANH, bool MOM>
+/* PT: storage and arithmetic type of the phase field (float, or double
+ * with the phase-field update -- selector terms, tanh, liquid fraction --
+ * evaluated in FP64). */
+template <typename PT>
+__device__ __forceinline__ PT tanh_pt(PT x, int mode);
+template <>
+__device__ __forceinline__ float tanh_pt<float>(float x, int mode) { return tanh_lp(x, mode); }
+template <>
+__device__ __forceinline__ double tanh_pt<double>(double x, int mode)
+{
+    return mode == BGK_TANH_PORTABLE ? bgk_portable_tanh(x) : tanh(x);
+}
+
+template <typename S, typename PT, int TANH, bool MOM>
 __global__ void __launch_bounds__(FUSED_BX)
-fused_lowp_kernel(LpPtrs<S> s, ConstsLP c, int H, int pf)
+fused_lowp_kernel(LpPtrs<S, PT> s, ConstsLP c, int H, int pf)
 {
     const int Nx = c.Nx, Ny = c.Ny;
     const int x = blockIdx.x * FUSED_BX + threadIdx.x;
@@ -173,18 +184,19 @@ fused_lowp_kernel(LpPtrs<S> s, ConstsLP c, int H, int pf)
     const bool W = (x == 0), E = (x == Nx - 1);
     const S *__restrict__ F = s.fin;
     const S *__restrict__ G = s.gin;
-    const float *__restrict__ PH = s.phin;
+    const PT *__restrict__ PH = s.phin;
     const float isf = s.inv_sf, isg = s.inv_sg;
 
-    float ap[3][3], am[3][3], pc[3];
+    PT ap[3][3], am[3][3], pc[3];
     auto load_row = [&](int r, int slot) {
         const int rc = r < 0 ? 0 : (r >= Ny ? Ny - 1 : r);
-        const float *row = PH + (long long)rc * P;
-        const float pL = W ? (float)s.phiW[rc] : row[x - 1];
-        const float pM = row[x];
-        const float pR = E ? (float)s.phiE[rc] : row[x + 1];
-        const float a0 = 0.5f * (1.0f + pL), a1 = 0.5f * (1.0f + pM), a2 = 0.5f * (1.0f + pR);
-        const float b0 = 0.5f * (1.0f - pL), b1 = 0.5f * (1.0f - pM), b2 = 0.5f * (1.0f - pR);
+        const PT *row = PH + (long long)rc * P;
+        const PT pL = W ? (PT)s.phiW[rc] : row[x - 1];
+        const PT pM = row[x];
+        const PT pR = E ? (PT)s.phiE[rc] : row[x + 1];
+        const PT h = (PT)0.5, one = (PT)1;
+        const PT a0 = h * (one + pL), a1 = h * (one + pM), a2 = h * (one + pR);
+        const PT b0 = h * (one - pL), b1 = h * (one - pM), b2 = h * (one - pR);
         ap[slot][0] = a0 * a0; ap[slot][1] = a1 * a1; ap[slot][2] = a2 * a2;
         am[slot][0] = b0 * b0; am[slot][1] = b1 * b1; am[slot][2] = b2 * b2;
         pc[slot] = pM;
@@ -246,17 +258,19 @@ fused_lowp_kernel(LpPtrs<S> s, ConstsLP c, int H, int pf)
         float v = irho * (f[2] - f[4] + f[5] + f[6] - f[7] - f[8]);
         const float dT2 = dT, u2 = u, v2 = v;
 
-        /* phase_field */
-        const float th = tanh_lp((c.T0mTcrit + dT) * c.inv_T_width, TANH);
-        const float kp = ap[1][1] + ap[1][2] + ap[2][1] + ap[1][0] + ap[0][1] + ap[2][2] + ap[2][0] + ap[0][0] + ap[0][2];
-        const float km = am[1][1] + am[1][2] + am[2][1] + am[1][0] + am[0][1] + am[2][2] + am[2][0] + am[0][0] + am[0][2];
-        const float p0 = pc[1];
-        const float kpp = kp * 0.125f * (0.5f * (1.0f + th));
-        const float kmm = km * 0.125f * (0.5f * (1.0f - th));
-        const float phn = p0 + (c.f_plus * kpp * (1.0f - p0) - c.f_minus * kmm * (1.0f + p0));
+        /* phase_field (in PT) */
+        const PT one = (PT)1, half = (PT)0.5;
+        const PT th = tanh_pt<PT>(((PT)c.T0mTcrit_d + (PT)dT) * (PT)c.inv_T_width_d, TANH);
+        const PT kp = ap[1][1] + ap[1][2] + ap[2][1] + ap[1][0] + ap[0][1] + ap[2][2] + ap[2][0] + ap[0][0] + ap[0][2];
+        const PT km = am[1][1] + am[1][2] + am[2][1] + am[1][0] + am[0][1] + am[2][2] + am[2][0] + am[0][0] + am[0][2];
+        const PT p0 = pc[1];
+        const PT kpp = kp * (PT)0.125 * (half * (one + th));
+        const PT kmm = km * (PT)0.125 * (half * (one - th));
+        const PT phn_p = p0 + (half * kpp * (one - p0) - half * kmm * (one + p0));
+        const float phn = (float)phn_p;
 
         /* forces: latent heat in FP64 */
-        dT = (float)((double)dT - c.dts * ((double)phn - (double)p0) * 0.5);
+        dT = (float)((double)dT - c.dts * ((double)phn_p - (double)p0) * 0.5);
         const float T = c.T0 + dT;
         const float omp = 1.0f - phn;
         const float forceY = rho * c.gb * T * (1.0f + 0.5f * phn) - 0.5f * v * omp;
@@ -278,7 +292,7 @@ fused_lowp_kernel(LpPtrs<S> s, ConstsLP c, int H, int pf)
         reg_relax_lp(c, g, eq, c.cg, out);
 #pragma unroll
         for (int k = 0; k < 9; k++) C::st(s.gout + k * pl + cc, out[k], s.sg);
-        s.phout[cc] = phn;
+        s.phout[cc] = phn_p;
 
         if (MOM || E) {
             float sg = 0.f;
@@ -299,7 +313,7 @@ fused_lowp_kernel(LpPtrs<S> s, ConstsLP c, int H, int pf)
                 s.mT[q] = Tm;
                 s.mu[q] = 0.5 * ((double)tu + (double)u2);
                 s.mv[q] = 0.5 * ((double)tv + (double)v2);
-                s.mphi[q] = (double)phn;
+                s.mphi[q] = (double)phn_p;
             }
         }
 #pragma unroll
@@ -313,8 +327,8 @@ fused_lowp_kernel(LpPtrs<S> s, ConstsLP c, int H, int pf)
 
 /* Initial condition in deviation storage (STEP_7/initialization.f90 with
  * the no-slip walls: u = v = u0 inside, 0 on rows 0 and Ny+1). */
-template <typename S>
-__global__ void init_lowp_kernel(Consts c, S *fd, S *gd, float *ph0, float *ph1, long long plane, int P,
+template <typename S, typename PT>
+__global__ void init_lowp_kernel(Consts c, S *fd, S *gd, PT *ph0, PT *ph1, long long plane, int P,
                                  float sf, float sg)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -330,7 +344,7 @@ __global__ void init_lowp_kernel(Consts c, S *fd, S *gd, float *ph0, float *ph1,
         Codec<S>::st(fd + k * plane + cc, (float)(c.w[k] * rho * Pq[k] - c.w[k] * c.rho0), sf);
         Codec<S>::st(gd + k * plane + cc, (float)(c.w[k] * T * Pq[k] - c.w[k] * c.T0), sg);
     }
-    const float phi = (i <= c.interf) ? 1.0f : -1.0f;
+    const PT phi = (i <= c.interf) ? (PT)1 : (PT)-1;
     ph0[cc] = phi;
     ph1[cc] = phi;
 }
@@ -391,19 +405,21 @@ ConstsLP make_lp(const bgk_ctx *b)
     l.gb = (float)(c.grav * c.beta);
     l.omega_f = (float)c.omega_f;
     l.dts = c.dts;
+    l.T0mTcrit_d = c.T0 - c.T_crit - c.T_act;
+    l.inv_T_width_d = 1.0 / c.T_width;
     l.T0d = c.T0;
     l.rho0d = c.rho0;
     return l;
 }
 
-template <typename S>
+template <typename S, typename PT>
 cudaError_t launch_lowp_t(bgk_ctx *c, bool moments)
 {
-    LpPtrs<S> s{};
+    LpPtrs<S, PT> s{};
     const int src = c->cur, dst = c->cur ^ 1;
     s.fin = (const S *)c->fbuf[src]; s.gin = (const S *)c->gbuf[src];
     s.fout = (S *)c->fbuf[dst]; s.gout = (S *)c->gbuf[dst];
-    s.phin = (const float *)c->phibuf[src]; s.phout = (float *)c->phibuf[dst];
+    s.phin = (const PT *)c->phibuf[src]; s.phout = (PT *)c->phibuf[dst];
     s.tcin = c->tcol[src]; s.tcout = c->tcol[dst];
     s.gW = c->gW; s.pE = c->pE; s.phiW = c->phiW; s.phiE = c->phiE; s.corner = c->corner;
     s.mrho = c->mrho; s.mT = c->mT; s.mu = c->mu; s.mv = c->mv; s.mphi = c->mphi;
@@ -412,13 +428,13 @@ cudaError_t launch_lowp_t(bgk_ctx *c, bool moments)
     const ConstsLP lp = make_lp(c);
     const int H = strip_height(c);
     dim3 grd((c->Nx + FUSED_BX - 1) / FUSED_BX, (c->Ny + H - 1) / H);
+#define BGK_LP(T, M) fused_lowp_kernel<S, PT, T, M><<<grd, FUSED_BX, 0, c->stream>>>(s, lp, H, c->tune_pf)
     if (c->opt.tanh_mode == BGK_TANH_PORTABLE) {
-        if (moments) fused_lowp_kernel<S, BGK_TANH_PORTABLE, true><<<grd, FUSED_BX, 0, c->stream>>>(s, lp, H, c->tune_pf);
-        else fused_lowp_kernel<S, BGK_TANH_PORTABLE, false><<<grd, FUSED_BX, 0, c->stream>>>(s, lp, H, c->tune_pf);
+        if (moments) BGK_LP(BGK_TANH_PORTABLE, true); else BGK_LP(BGK_TANH_PORTABLE, false);
     } else {
-        if (moments) fused_lowp_kernel<S, BGK_TANH_DEVICE, true><<<grd, FUSED_BX, 0, c->stream>>>(s, lp, H, c->tune_pf);
-        else fused_lowp_kernel<S, BGK_TANH_DEVICE, false><<<grd, FUSED_BX, 0, c->stream>>>(s, lp, H, c->tune_pf);
+        if (moments) BGK_LP(BGK_TANH_DEVICE, true); else BGK_LP(BGK_TANH_DEVICE, false);
     }
+#undef BGK_LP
     return cudaGetLastError();
 }
 
@@ -426,8 +442,10 @@ cudaError_t launch_lowp_t(bgk_ctx *c, bool moments)
 
 cudaError_t launch_fused_lowp(bgk_ctx *c, bool moments)
 {
-    if (c->opt.precision == BGK_PREC_F32) return launch_lowp_t<float>(c, moments);
-    return launch_lowp_t<__half>(c, moments);
+    const bool p64 = c->phisz == 8;
+    if (c->opt.precision == BGK_PREC_F32)
+        return p64 ? launch_lowp_t<float, double>(c, moments) : launch_lowp_t<float, float>(c, moments);
+    return p64 ? launch_lowp_t<__half, double>(c, moments) : launch_lowp_t<__half, float>(c, moments);
 }
 
 /* FP16 scales: powers of two that put the largest deviations expected in
@@ -461,13 +479,17 @@ cudaError_t launch_init_lowp(bgk_ctx *c)
     c->gbuf[c->cur] = gb;
     if (e != cudaSuccess) return e;
     dim3 blk(32, 8), grd((c->Nx + 31) / 32, (c->Ny + 7) / 8);
-    if (c->opt.precision == BGK_PREC_F32)
-        init_lowp_kernel<float><<<grd, blk, 0, c->stream>>>(c->c, (float *)fb, (float *)gb, (float *)c->phibuf[0],
-                                                            (float *)c->phibuf[1], c->plane, c->P, 1.f, 1.f);
-    else
-        init_lowp_kernel<__half><<<grd, blk, 0, c->stream>>>(c->c, (__half *)fb, (__half *)gb, (float *)c->phibuf[0],
-                                                             (float *)c->phibuf[1], c->plane, c->P, c->scale.sf,
-                                                             c->scale.sg);
+    const bool p64 = c->phisz == 8;
+#define BGK_INIT(S, PT, sf_, sg_)                                                                        \
+    init_lowp_kernel<S, PT><<<grd, blk, 0, c->stream>>>(c->c, (S *)fb, (S *)gb, (PT *)c->phibuf[0],     \
+                                                        (PT *)c->phibuf[1], c->plane, c->P, sf_, sg_)
+    if (c->opt.precision == BGK_PREC_F32) {
+        if (p64) BGK_INIT(float, double, 1.f, 1.f); else BGK_INIT(float, float, 1.f, 1.f);
+    } else {
+        if (p64) BGK_INIT(__half, double, c->scale.sf, c->scale.sg);
+        else BGK_INIT(__half, float, c->scale.sf, c->scale.sg);
+    }
+#undef BGK_INIT
     return cudaGetLastError();
 }
 
@@ -489,8 +511,13 @@ static int lp_to_compact(bgk_ctx *c, int field, const double *ref)
         lp_ref_to_plane<S><<<grd, blk, 0, c->stream>>>(c->c, ref, (S *)c->gbuf[c->cur] + k * c->plane, c->P,
                                                        c->c.w[k] * c->c.T0, c->scale.sg);
     } else if (field == BGK_FIELD_PHI) {
-        lp_ref_to_plane<float><<<grd, blk, 0, c->stream>>>(c->c, ref, (float *)c->phibuf[0], c->P, 0.0, 1.f);
-        lp_ref_to_plane<float><<<grd, blk, 0, c->stream>>>(c->c, ref, (float *)c->phibuf[1], c->P, 0.0, 1.f);
+        if (c->phisz == 8) {
+            lp_ref_to_plane<double><<<grd, blk, 0, c->stream>>>(c->c, ref, (double *)c->phibuf[0], c->P, 0.0, 1.f);
+            lp_ref_to_plane<double><<<grd, blk, 0, c->stream>>>(c->c, ref, (double *)c->phibuf[1], c->P, 0.0, 1.f);
+        } else {
+            lp_ref_to_plane<float><<<grd, blk, 0, c->stream>>>(c->c, ref, (float *)c->phibuf[0], c->P, 0.0, 1.f);
+            lp_ref_to_plane<float><<<grd, blk, 0, c->stream>>>(c->c, ref, (float *)c->phibuf[1], c->P, 0.0, 1.f);
+        }
     } else if (field == BGK_FIELD_T) {
         lp_tcol_kernel<<<(c->Ny + 127) / 128, 128, 0, c->stream>>>(c->c, ref, c->tcol[c->cur]);
     } else if (field != BGK_FIELD_RHO && field != BGK_FIELD_U && field != BGK_FIELD_V) {
@@ -515,8 +542,12 @@ static int lp_to_ref(bgk_ctx *c, int field, double *ref, int prev)
         lp_plane_to_ref<S><<<grd, blk, 0, c->stream>>>(c->c, (const S *)c->gbuf[b] + k * c->plane, c->P, ref,
                                                        c->c.w[k] * c->c.T0, c->scale.inv_sg, nullptr, -1, -1, nullptr);
     } else if (field == BGK_FIELD_PHI_PREC) {
-        lp_plane_to_ref<float><<<grd, blk, 0, c->stream>>>(c->c, (const float *)c->phibuf[b], c->P, ref, 0.0, 1.f,
-                                                           c->mphi, -1, -1, nullptr);
+        if (c->phisz == 8)
+            lp_plane_to_ref<double><<<grd, blk, 0, c->stream>>>(c->c, (const double *)c->phibuf[b], c->P, ref, 0.0,
+                                                                1.f, c->mphi, -1, -1, nullptr);
+        else
+            lp_plane_to_ref<float><<<grd, blk, 0, c->stream>>>(c->c, (const float *)c->phibuf[b], c->P, ref, 0.0, 1.f,
+                                                               c->mphi, -1, -1, nullptr);
     } else {
         return BGK_ERR_UNSUPPORTED;
     }

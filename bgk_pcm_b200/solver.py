@@ -31,14 +31,14 @@ class Solver:
     """One simulation on one B200 (STEP_7/setup.f90 allocates, this creates)."""
 
     def __init__(self, params, precision: str = "f64", tanh: str = "device", fma: bool = False,
-                 device: int = -1):
+                 device: int = -1, smooth: bool = False):
         lib = capi.load()
         if isinstance(params, dict):
             params = capi.Params.from_dict(params)
         self.params = params
         self.Nx, self.Ny = params.Nx, params.Ny
         self.precision = precision
-        opt = capi.Options(_PREC[precision], _TANH[tanh], 1 if fma else 0, device)
+        opt = capi.Options(_PREC[precision], _TANH[tanh], 1 if fma else 0, device, 1 if smooth else 0)
         h = ctypes.c_void_p()
         capi.check(lib.bgk_create(ctypes.byref(params), ctypes.byref(opt), ctypes.byref(h)))
         self._h = h

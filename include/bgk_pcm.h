@@ -67,6 +67,11 @@ typedef struct bgk_options {
     int fma;         /* FP64 only: 0 = the reference's exact operation order    */
                      /* (no fused multiply-add); 1 = FMA-contracted variant      */
     int device;      /* CUDA device ordinal, or -1 for the current device        */
+    int smooth;      /* FP64 only: 0 = the reference's roundings, including the  */
+                     /* REAL(4) temporaries ft0..ft8 / gt0..gt8 of               */
+                     /* STEP_7/collision.f90:84-120 (implicitly typed); 1 = keep */
+                     /* them in double, which makes the step a smooth function   */
+                     /* of its inputs (the form the adjoint differentiates)      */
 } bgk_options;
 
 /* ----------------------------------------------------------------- fields */

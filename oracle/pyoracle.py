@@ -61,6 +61,7 @@ def load() -> ctypes.CDLL:
         getattr(lib, n).restype = None
     lib.orc_step.argtypes = [vp, ctypes.c_int]
     lib.orc_set_tanh_mode.argtypes = [vp, ctypes.c_int]
+    lib.orc_set_smooth.argtypes = [vp, ctypes.c_int]
     lib.orc_set_threads.argtypes = [ctypes.c_int]
     lib.orc_get_it.argtypes = [vp]
     lib.orc_set_it.argtypes = [vp, ctypes.c_int]
@@ -87,7 +88,7 @@ class Oracle:
 
     STAGES = ("bc_f", "bc_g", "streaming", "moments_pre", "phase_field", "forces", "collision", "moments")
 
-    def __init__(self, params: dict, tanh: str = "libm", threads: int = 0):
+    def __init__(self, params: dict, tanh: str = "libm", threads: int = 0, smooth: bool = False):
         self.lib = load()
         p = OrcParams()
         for n, _ in OrcParams._fields_:
@@ -99,6 +100,7 @@ class Oracle:
         if not self.h:
             raise ValueError("orc_create failed")
         self.lib.orc_set_tanh_mode(self.h, 1 if tanh == "portable" else 0)
+        self.lib.orc_set_smooth(self.h, 1 if smooth else 0)
 
     def close(self):
         if self.h:

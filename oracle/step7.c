@@ -62,6 +62,7 @@ struct orc_state {
     int westBC, eastBC, northBC, southBC;
     int deltaOut, itOut;
     int tanh_mode;
+    int smooth;            /* 1: keep ft/gt in double (the differentiable form) */
     /* diag.f90's melt_front/melt_front_expected are locals that are not
      * assigned on every path; they are carried from call to call here. */
     double diag_melt_front, diag_melt_front_expected;
@@ -222,6 +223,7 @@ void orc_destroy(orc_state *s)
 }
 
 void orc_set_tanh_mode(orc_state *s, int mode) { s->tanh_mode = mode; }
+void orc_set_smooth(orc_state *s, int smooth) { s->smooth = smooth; }
 double *orc_field(orc_state *s, int id) { return (id >= 0 && id < ORC_NFIELDS) ? s->fld[id] : NULL; }
 int orc_get_it(const orc_state *s) { return s->it; }
 void orc_set_it(orc_state *s, int it) { s->it = it; }
@@ -664,6 +666,33 @@ void orc_collision(orc_state *s)
             gt[6] = ge[6] + C[6] * (q1 * txx + q1 * tyy - 2.0 * txy);
             gt[7] = ge[7] + C[7] * (q1 * txx + q1 * tyy + 2.0 * txy);
             gt[8] = ge[8] + C[8] * (q1 * txx + q1 * tyy - 2.0 * txy);
+            if (s->smooth) {
+                /* the differentiable form: ft/gt kept in double */
+                double fd[9], gd[9];
+                fd[0] = fe[0] + C[0] * (m * pxx + m * pyy);
+                fd[1] = fe[1] + C[1] * (q1 * pxx + m * pyy);
+                fd[2] = fe[2] + C[2] * (m * pxx + q1 * pyy);
+                fd[3] = fe[3] + C[3] * (q1 * pxx + m * pyy);
+                fd[4] = fe[4] + C[4] * (m * pxx + q1 * pyy);
+                fd[5] = fe[5] + C[5] * (q1 * pxx + q1 * pyy + 2.0 * pxy);
+                fd[6] = fe[6] + C[6] * (q1 * pxx + q1 * pyy - 2.0 * pxy);
+                fd[7] = fe[7] + C[7] * (q1 * pxx + q1 * pyy + 2.0 * pxy);
+                fd[8] = fe[8] + C[8] * (q1 * pxx + q1 * pyy - 2.0 * pxy);
+                gd[0] = ge[0] + C[0] * (m * txx + m * tyy);
+                gd[1] = ge[1] + C[1] * (q1 * txx + m * tyy);
+                gd[2] = ge[2] + C[2] * (m * txx + q1 * tyy);
+                gd[3] = ge[3] + C[3] * (q1 * txx + m * tyy);
+                gd[4] = ge[4] + C[4] * (m * txx + q1 * tyy);
+                gd[5] = ge[5] + C[5] * (q1 * txx + q1 * tyy + 2.0 * txy);
+                gd[6] = ge[6] + C[6] * (q1 * txx + q1 * tyy - 2.0 * txy);
+                gd[7] = ge[7] + C[7] * (q1 * txx + q1 * tyy + 2.0 * txy);
+                gd[8] = ge[8] + C[8] * (q1 * txx + q1 * tyy - 2.0 * txy);
+                for (int k = 0; k < 9; k++) {
+                    F(k)[q] = fd[k] - omf * (fd[k] - fe[k]);
+                    G(k)[q] = gd[k] - omg * (gd[k] - ge[k]);
+                }
+                continue;
+            }
             for (int k = 0; k < 9; k++) {
                 F(k)[q] = (double)ft[k] - omf * ((double)ft[k] - fe[k]);
                 G(k)[q] = (double)gt[k] - omg * ((double)gt[k] - ge[k]);

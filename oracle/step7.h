@@ -57,6 +57,9 @@ void orc_destroy(orc_state *s);
 
 /* 0 = libm tanh (as the reference), 1 = bgk_portable_tanh (bit-exact mode). */
 void orc_set_tanh_mode(orc_state *s, int mode);
+/* 1 = keep collision.f90's ft/gt temporaries in double (the smooth,
+ * differentiable form); 0 = their implicit REAL(4) (the reference). */
+void orc_set_smooth(orc_state *s, int smooth);
 /* OpenMP threads for the hot loops (0 = leave the runtime default). */
 void orc_set_threads(int n);
 

@@ -40,6 +40,7 @@ def test_fp32_form_within_1e4(lib):
     ref = run("f64", p, 3000)
     lo = run("f32", p, 3000)
     e = errors(ref, lo, p)
+    print("fp32 form errors", e)
     assert e["T"] <= 1e-4 and e["phi"] <= 1e-4, e
     assert e["u"] <= 1e-2 and e["v"] <= 1e-2, e
 
