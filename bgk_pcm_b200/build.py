@@ -28,6 +28,7 @@ UNITS = {
     "kernels_f64.cu": ["--fmad=false"],
     "kernels_fast.cu": ["--fmad=true"],
     "capi.cu": ["--fmad=false"],
+    "adjoint.cu": ["--fmad=true"],
 }
 
 

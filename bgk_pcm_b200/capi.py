@@ -47,7 +47,7 @@ EXPORTS = [
     "bgk_step", "bgk_bc_f", "bgk_bc_g", "bgk_streaming", "bgk_moments_pre",
     "bgk_phase_field", "bgk_forces", "bgk_collision", "bgk_moments", "bgk_upload",
     "bgk_download", "bgk_download_region", "bgk_field_sums", "bgk_get_it", "bgk_set_it",
-    "bgk_set_tin", "bgk_sync", "bgk_get_stream", "bgk_save", "bgk_load",
+    "bgk_set_tin", "bgk_sync", "bgk_get_stream", "bgk_save", "bgk_load", "bgk_adjoint_run",
 ]
 
 
@@ -75,6 +75,12 @@ class Params(ctypes.Structure):
 class Options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("tanh_mode", ctypes.c_int), ("fma", ctypes.c_int),
                 ("device", ctypes.c_int), ("smooth", ctypes.c_int)]
+
+
+class AdjointSpec(ctypes.Structure):
+    _fields_ = [("nsteps", ctypes.c_int), ("checkpoint_every", ctypes.c_int), ("nprobes", ctypes.c_int),
+                ("probe_i", ctypes.POINTER(ctypes.c_int)), ("probe_j", ctypes.POINTER(ctypes.c_int)),
+                ("phi_target", ctypes.POINTER(ctypes.c_double))]
 
 
 class BGKError(RuntimeError):
@@ -116,6 +122,7 @@ def load() -> ctypes.CDLL:
         "bgk_get_stream": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_void_p)]),
         "bgk_save": (ctypes.c_int, [P, ctypes.c_char_p]),
         "bgk_load": (ctypes.c_int, [P, ctypes.c_char_p]),
+        "bgk_adjoint_run": (ctypes.c_int, [P, ctypes.POINTER(AdjointSpec), dp, dp, dp]),
     }
     for n in ("bgk_bc_f", "bgk_bc_g", "bgk_streaming", "bgk_moments_pre", "bgk_phase_field",
               "bgk_forces", "bgk_collision", "bgk_moments"):

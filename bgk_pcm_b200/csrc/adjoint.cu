@@ -1,0 +1,528 @@
+/*
+ * adjoint.cu -- the differentiation form: a hand-written reverse of the fused
+ * FP64 step (smooth form, see bgk_options.smooth) run backward in time with
+ * checkpoint-and-recompute.
+ *
+ * One reverse step (forward step n: S(n-1) -> S(n)) is one kernel, fused in
+ * gather form.  At node i it
+ *  1. gathers the adjoint of the state S(n) at i -- lambda_f[k], lambda_g[k],
+ *     lambda_phi and (east column) lambda of T(Nx, y) -- from the local
+ *     partials Pi(n+1) that the reverse of step n+1 left at the nodes that
+ *     read those values: the node that pulled the population (i + c_k), the
+ *     node itself when the pull was a bounce-back, the rows that read a
+ *     clamped (copied) halo row of g or phi, and the 3x3 stencils that read
+ *     phi(i);
+ *  2. recomputes the forward node update of step n from S(n-1);
+ *  3. applies the vector-Jacobian product of that update and stores the
+ *     partials Pi(n)(i): the adjoints of the 18 pulled populations, of the
+ *     two 3x3 selector sums (k+, k-) and of phi_prec(i).
+ * Each step therefore reads S(n-1) and Pi(n+1) once and writes Pi(n) once.
+ * Parameter gradients: d/d omega_g per block (deterministic partial sums),
+ * d/dTin per row from the west nodes' pulled-g partials.
+ *
+ * Forward states come from snapshots every K steps; each K-step segment is
+ * recomputed with the fused kernel before it is reversed.
+ */
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "bgk_internal.h"
+#include "bgk_math.cuh"
+#include "../../include/bgk_portable_tanh.h"
+
+namespace {
+
+using bgk::Consts;
+
+constexpr int NPI = 21;          /* partial planes: f[9], g[9], k+, k-, phi_prec */
+constexpr int AB_X = 64, AB_Y = 4;
+
+__constant__ int d_cx[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
+__constant__ int d_cy[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
+__constant__ int d_opp[9] = {0, 3, 4, 1, 2, 7, 8, 5, 6};
+/* A_k, B_k, E_k of S_k = A_k Pxx + B_k Pyy + 2 E_k Pxy (collision.f90:84-100);
+ * the same coefficients weight d_k in Pxx, Pyy, Pxy. */
+__constant__ int d_AisQ[9] = {0, 1, 0, 1, 0, 1, 1, 1, 1};
+__constant__ int d_BisQ[9] = {0, 0, 1, 0, 1, 1, 1, 1, 1};
+__constant__ double d_E[9] = {0, 0, 0, 0, 0, 1, -1, 1, -1};
+
+struct AdjPtrs {
+    const double *f, *g, *phi, *tcol;      /* state S(n-1), compact          */
+    const double *pin;                     /* Pi(n+1): NPI planes            */
+    double *pout;                          /* Pi(n)                          */
+    const double *gW, *pE, *phiW, *phiE, *corner;
+    double *omg_acc;                       /* per-block running sums         */
+    long long plane;
+    int P;
+    int tanh_mode;
+};
+
+__device__ __forceinline__ double tanh_sel(double x, int mode)
+{
+    return mode == BGK_TANH_PORTABLE ? bgk_portable_tanh(x) : tanh(x);
+}
+
+/* dP_k/du and dP_k/dv of the equilibrium polynomials (see eq_poly). */
+__device__ __forceinline__ void eq_poly_grad(double u, double v, double *du, double *dv)
+{
+    const double upv = u + v, umv = u - v;
+    du[0] = -3.0 * u;                     dv[0] = -3.0 * v;
+    du[1] = 3.0 + 6.0 * u;                dv[1] = -3.0 * v;
+    du[2] = -3.0 * u;                     dv[2] = 3.0 + 6.0 * v;
+    du[3] = -3.0 + 6.0 * u;               dv[3] = -3.0 * v;
+    du[4] = -3.0 * u;                     dv[4] = -3.0 + 6.0 * v;
+    du[5] = 3.0 + 9.0 * upv - 3.0 * u;    dv[5] = 3.0 + 9.0 * upv - 3.0 * v;
+    du[6] = -3.0 + 9.0 * umv - 3.0 * u;   dv[6] = 3.0 - 9.0 * umv - 3.0 * v;
+    du[7] = -3.0 + 9.0 * upv - 3.0 * u;   dv[7] = -3.0 + 9.0 * upv - 3.0 * v;
+    du[8] = 3.0 + 9.0 * umv - 3.0 * u;    dv[8] = -3.0 - 9.0 * umv - 3.0 * v;
+}
+
+/* Vector-Jacobian product of one node update (smooth form).
+ * in : pulled f, g; selector sums kp, km; phi_prec p0; output adjoints
+ *      Fo_b (f post-collision), Go_b (g post-collision), phn_b (new phi),
+ *      Tm_b (moments T written for the east boundary).
+ * out: f_b, g_b (pulled), kp_b, km_b, p0_b, omg_b (d/d omega_g). */
+__device__ void node_vjp(const Consts &c, int tanh_mode, const double *f, const double *g, double kp, double km,
+                         double p0, const double *Fo_b, const double *Go_b, double phn_b, double Tm_b, double *f_b,
+                         double *g_b, double &kp_b, double &km_b, double &p0_b, double &omg_b)
+{
+    const double m = c.m_cs2, q = c.q_cs2;
+    /* ---- forward recompute ---- */
+    double rho = 0.0, T = 0.0;
+#pragma unroll
+    for (int k = 0; k < 9; k++) { rho += f[k]; T += g[k]; }
+    const double irho = 1.0 / rho;
+    const double mx = f[1] - f[3] + f[5] - f[6] - f[7] + f[8];
+    const double my = f[2] - f[4] + f[5] + f[6] - f[7] - f[8];
+    const double u = irho * mx, v = irho * my;
+    const double arg = ((T - c.T_crit) - c.T_act) / c.T_width;
+    const double th = tanh_sel(arg, tanh_mode);
+    const double rp = 0.5 * (1.0 + th), rm = 0.5 * (1.0 - th);
+    const double KP = (kp / 8.0) * rp, KM = (km / 8.0) * rm;
+    const double phn = p0 + (c.f_plus * KP * (1.0 - p0) - c.f_minus * KM * (1.0 + p0));
+    const double Tf = T - c.dts * (phn - p0) / 2.0;
+    const double gb = c.grav * c.beta;
+    const double onep = 1.0 + phn / 2.0;
+    const double FY0 = rho * gb * Tf * onep;
+    const double omp = 1.0 - phn;
+    const double FX = -(u * omp * 0.5);
+    const double FY = FY0 - v * omp * 0.5;
+    const double orho = c.omega_f * rho;
+    const double uf = u + FX / orho, vf = v + FY / orho;
+    double Pq[9], dPu[9], dPv[9];
+    bgk::eq_poly(uf, vf, Pq);
+    eq_poly_grad(uf, vf, dPu, dPv);
+    double e[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) e[k] = g[k] - c.w[k] * Tf * Pq[k];
+    double txx = 0.0, tyy = 0.0, txy = 0.0;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        txx += (d_AisQ[k] ? q : m) * e[k];
+        tyy += (d_BisQ[k] ? q : m) * e[k];
+        txy += d_E[k] * e[k];
+    }
+
+    /* ---- reverse ---- */
+    double Gob[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) Gob[k] = Go_b[k] + 0.5 * Tm_b;
+    /* g collision: go_k = geq_k + (1-omega_g) C_k Sg_k */
+    const double cg = 1.0 - c.omega_g, cf = 1.0 - c.omega_f;
+    double txxb = 0.0, tyyb = 0.0, txyb = 0.0, pxxb = 0.0, pyyb = 0.0, pxyb = 0.0;
+    omg_b = 0.0;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        const double A = d_AisQ[k] ? q : m, B = d_BisQ[k] ? q : m;
+        const double Sg = A * txx + B * tyy + 2.0 * d_E[k] * txy;
+        omg_b += Gob[k] * (-c.C[k] * Sg);
+        const double sb = Gob[k] * cg * c.C[k];
+        txxb += sb * A; tyyb += sb * B; txyb += 2.0 * sb * d_E[k];
+        const double sf = Fo_b[k] * cf * c.C[k];
+        pxxb += sf * A; pyyb += sf * B; pxyb += 2.0 * sf * d_E[k];
+    }
+    double rhob = 0.0, Tfb = 0.0, ufb = 0.0, vfb = 0.0;
+#pragma unroll
+    for (int j = 0; j < 9; j++) {
+        const double A = d_AisQ[j] ? q : m, B = d_BisQ[j] ? q : m;
+        const double eb = A * txxb + B * tyyb + d_E[j] * txyb;
+        const double db = A * pxxb + B * pyyb + d_E[j] * pxyb;
+        g_b[j] = eb;
+        f_b[j] = db;
+        const double geqb = Gob[j] - eb;
+        const double feqb = Fo_b[j] - db;
+        rhob += feqb * c.w[j] * Pq[j];
+        Tfb += geqb * c.w[j] * Pq[j];
+        const double Pb = c.w[j] * (feqb * rho + geqb * Tf);
+        ufb += Pb * dPu[j];
+        vfb += Pb * dPv[j];
+    }
+    /* velocity shift */
+    double ub = ufb, vb = vfb;
+    const double FXb = ufb / orho, FYb = vfb / orho;
+    const double orhob = -(ufb * FX + vfb * FY) / (orho * orho);
+    rhob += c.omega_f * orhob;
+    /* drag and buoyancy */
+    const double FY0b = FYb;
+    vb += -0.5 * omp * FYb;
+    double phnb = 0.5 * v * FYb;
+    ub += -0.5 * omp * FXb;
+    phnb += 0.5 * u * FXb;
+    rhob += FY0b * gb * Tf * onep;
+    Tfb += FY0b * rho * gb * onep;
+    phnb += FY0b * rho * gb * Tf * 0.5;
+    /* latent heat */
+    double Tb = Tfb;
+    phnb += -0.5 * c.dts * Tfb;
+    p0_b = 0.5 * c.dts * Tfb;
+    /* phase field */
+    const double PHb = phn_b + phnb;
+    p0_b += PHb * (1.0 - c.f_plus * KP - c.f_minus * KM);
+    const double KPb = PHb * c.f_plus * (1.0 - p0);
+    const double KMb = -PHb * c.f_minus * (1.0 + p0);
+    kp_b = KPb * rp / 8.0;
+    km_b = KMb * rm / 8.0;
+    const double rpb = KPb * kp / 8.0, rmb = KMb * km / 8.0;
+    const double thb = 0.5 * rpb - 0.5 * rmb;
+    Tb += thb * (1.0 - th * th) / c.T_width;
+    Tb += 0.5 * Tm_b;
+    /* momentsPre */
+    const double mxb = ub * irho, myb = vb * irho;
+    const double irhob = ub * mx + vb * my;
+    rhob += -irhob * irho * irho;
+#pragma unroll
+    for (int j = 0; j < 9; j++) {
+        f_b[j] += rhob + d_cx[j] * mxb + d_cy[j] * myb;
+        g_b[j] += Tb;
+    }
+}
+
+__device__ __forceinline__ double PI(const AdjPtrs &s, int k, int x, int y)
+{
+    return s.pin[k * s.plane + (long long)y * s.P + x];
+}
+
+__global__ void __launch_bounds__(AB_X *AB_Y)
+adj_step_kernel(AdjPtrs s, Consts c)
+{
+    const int Nx = c.Nx, Ny = c.Ny;
+    const int x = blockIdx.x * AB_X + threadIdx.x;
+    const int y = blockIdx.y * AB_Y + threadIdx.y;
+    const bool active = x < Nx && y < Ny;
+    double omg_b = 0.0;
+    if (active) {
+        const long long pl = s.plane;
+        const int P = s.P;
+        const long long cc = (long long)y * P + x;
+        const bool W = x == 0, E = x == Nx - 1, S = y == 0, N = y == Ny - 1;
+
+        /* 1. gather the adjoint of S(n) at this node */
+        double lf[9], lg[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            const int xd = x + d_cx[k], yd = y + d_cy[k];
+            if (xd >= 0 && xd < Nx && yd >= 0 && yd < Ny) {
+                lf[k] = PI(s, k, xd, yd);
+            } else {
+                /* read by this node's own bounce-back of opp(k), except the
+                 * two frozen corners (pop 6 at (Nx,1), pop 7 at (Nx,Ny)) */
+                const bool corner6 = (k == 8) && E && S;
+                const bool corner7 = (k == 5) && E && N;
+                lf[k] = (corner6 || corner7) ? 0.0 : PI(s, d_opp[k], x, y);
+            }
+            double a = 0.0;
+            if (xd >= 0 && xd < Nx) {
+                if (yd >= 0 && yd < Ny) a += PI(s, 9 + k, xd, yd);
+                if (d_cy[k] == 1 && y == 0) a += PI(s, 9 + k, xd, 0);
+                if (d_cy[k] == -1 && y == Ny - 1) a += PI(s, 9 + k, xd, Ny - 1);
+            }
+            lg[k] = a;
+        }
+        /* phi: own direct partial + the 3x3 stencils that read this cell */
+        double skp = 0.0, skm = 0.0;
+        for (int dy = -1; dy <= 1; dy++) {
+            for (int dx = -1; dx <= 1; dx++) {
+                const int xd = x - dx;
+                if (xd < 0 || xd >= Nx) continue;
+                const int yd = y - dy;
+                if (yd >= 0 && yd < Ny) { skp += PI(s, 18, xd, yd); skm += PI(s, 19, xd, yd); }
+                if (dy == -1 && y == 0) { skp += PI(s, 18, xd, 0); skm += PI(s, 19, xd, 0); }
+                if (dy == 1 && y == Ny - 1) { skp += PI(s, 18, xd, Ny - 1); skm += PI(s, 19, xd, Ny - 1); }
+            }
+        }
+        const double ph = s.phi[cc];
+        const double lphi = PI(s, 20, x, y) + 0.5 * (1.0 + ph) * skp - 0.5 * (1.0 - ph) * skm;
+        /* T(Nx, y) written by this (east) node: read by the east pulls of
+         * pops 3 (same row), 6 (row y+1, or row 0 itself) and 7 (row y-1, or
+         * row Ny-1 itself) of the next step */
+        double lT = 0.0;
+        if (E) {
+            lT += PI(s, 9 + 3, x, y) * c.w[3] * s.pE[y];
+            double a6 = 0.0, a7 = 0.0;
+            if (y + 1 < Ny) a6 += PI(s, 9 + 6, x, y + 1);
+            if (y == 0) a6 += PI(s, 9 + 6, x, 0);
+            if (y - 1 >= 0) a7 += PI(s, 9 + 7, x, y - 1);
+            if (y == Ny - 1) a7 += PI(s, 9 + 7, x, Ny - 1);
+            lT += a6 * c.w[6] * s.pE[Ny + y] + a7 * c.w[7] * s.pE[2 * Ny + y];
+        }
+
+        /* 2. pulled inputs of step n from S(n-1) (as fused_f64_kernel) */
+        const double *F = s.f, *G = s.g;
+        double f[9], g[9];
+        f[0] = F[cc];
+        f[1] = *(W ? F + 3 * pl + cc : F + 1 * pl + cc - 1);
+        f[2] = *(S ? F + 4 * pl + cc : F + 2 * pl + cc - P);
+        f[3] = *(E ? F + 1 * pl + cc : F + 3 * pl + cc + 1);
+        f[4] = *(N ? F + 2 * pl + cc : F + 4 * pl + cc + P);
+        f[5] = *((W || S) ? F + 7 * pl + cc : F + 5 * pl + cc - P - 1);
+        f[6] = *((E || S) ? F + 8 * pl + cc : F + 6 * pl + cc - P + 1);
+        f[7] = *((E || N) ? F + 5 * pl + cc : F + 7 * pl + cc + P + 1);
+        f[8] = *((W || N) ? F + 6 * pl + cc : F + 8 * pl + cc + P - 1);
+        if (E && S) f[6] = s.corner[0];
+        if (E && N) f[7] = s.corner[1];
+        const int ym = S ? y : y - 1, yp = N ? y : y + 1;
+        const long long cm = (long long)ym * P + x, cp = (long long)yp * P + x;
+        g[0] = G[cc];
+        g[1] = *(W ? s.gW + y : G + 1 * pl + cc - 1);
+        g[2] = G[2 * pl + cm];
+        g[4] = G[4 * pl + cp];
+        g[5] = *(W ? s.gW + Ny + ym : G + 5 * pl + cm - 1);
+        g[8] = *(W ? s.gW + 2 * Ny + yp : G + 8 * pl + cp - 1);
+        if (E) {
+            g[3] = c.w[3] * s.tcol[y] * s.pE[y];
+            g[6] = c.w[6] * s.tcol[ym] * s.pE[Ny + ym];
+            g[7] = c.w[7] * s.tcol[yp] * s.pE[2 * Ny + yp];
+        } else {
+            g[3] = G[3 * pl + cc + 1];
+            g[6] = G[6 * pl + cm + 1];
+            g[7] = G[7 * pl + cp + 1];
+        }
+        double kp = 0.0, km = 0.0;
+        for (int dy = -1; dy <= 1; dy++) {
+            const int r = min(max(y + dy, 0), Ny - 1);
+            for (int dx = -1; dx <= 1; dx++) {
+                const int xs = x + dx;
+                const double p = xs < 0 ? s.phiW[r] : (xs >= Nx ? s.phiE[r] : s.phi[(long long)r * P + xs]);
+                kp += bgk::aplus(p);
+                km += bgk::aminus(p);
+            }
+        }
+
+        /* 3. vector-Jacobian product -> Pi(n) */
+        double fb[9], gbv[9], kpb, kmb, p0b;
+        node_vjp(c, s.tanh_mode, f, g, kp, km, ph, lf, lg, lphi, lT, fb, gbv, kpb, kmb, p0b, omg_b);
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            s.pout[k * pl + cc] = fb[k];
+            s.pout[(9 + k) * pl + cc] = gbv[k];
+        }
+        s.pout[18 * pl + cc] = kpb;
+        s.pout[19 * pl + cc] = kmb;
+        s.pout[20 * pl + cc] = p0b;
+    }
+    /* deterministic per-block accumulation of d/d omega_g */
+    __shared__ double red[AB_X * AB_Y];
+    const int t = threadIdx.y * AB_X + threadIdx.x;
+    red[t] = omg_b;
+    __syncthreads();
+    for (int o = AB_X * AB_Y / 2; o > 0; o >>= 1) {
+        if (t < o) red[t] += red[t + o];
+        __syncthreads();
+    }
+    if (t == 0) s.omg_acc[blockIdx.y * gridDim.x + blockIdx.x] += red[0];
+}
+
+/* dL/dTin per row from the west nodes' pulled-g partials of one step:
+ * pop 1 reads the west value of its own row, pop 5 that of row y-1
+ * (clamped), pop 8 that of row y+1 (clamped). */
+__global__ void adj_tin_kernel(const double *pi, long long plane, int P, int Ny, const double *dgW, double *grad)
+{
+    for (int y = threadIdx.x; y < Ny; y += blockDim.x) {
+        auto at = [&](int k, int yy) { return pi[(9 + k) * plane + (long long)yy * P]; };
+        double a = at(1, y) * dgW[y];
+        double b5 = 0.0, b8 = 0.0;
+        if (y + 1 < Ny) b5 += at(5, y + 1);
+        if (y == 0) b5 += at(5, 0);
+        if (y - 1 >= 0) b8 += at(8, y - 1);
+        if (y == Ny - 1) b8 += at(8, Ny - 1);
+        a += b5 * dgW[Ny + y] + b8 * dgW[2 * Ny + y];
+        grad[y] += a;
+    }
+}
+
+/* d gW_k / d Tin = w_k * poly_k(u(0,j), v(0,j)) for k = 1, 5, 8 */
+__global__ void adj_dgw_kernel(Consts c, const double *mu, const double *mv, double *dgW)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (j > c.Ny) return;
+    const size_t q = (size_t)(c.Nx + 2) * j;
+    double P[9];
+    bgk::eq_poly(mu[q], mv[q], P);
+    dgW[j - 1] = c.w[1] * P[1];
+    dgW[c.Ny + j - 1] = c.w[5] * P[5];
+    dgW[2 * c.Ny + j - 1] = c.w[8] * P[8];
+}
+
+/* Loss and its seed: Pi(N+1)[phi_prec] = 2 (phi - target) at the probes
+ * (serial, so repeated probes add deterministically). */
+__global__ void adj_seed_kernel(const double *phi, long long plane, int P, int np, const int *pi_, const int *pj,
+                                const double *target, double *seed_plane, double *loss)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double L = 0.0;
+    for (int p = 0; p < np; p++) {
+        const long long q = (long long)(pj[p] - 1) * P + (pi_[p] - 1);
+        const double r = phi[q] - target[p];
+        L += r * r;
+        seed_plane[q] += 2.0 * r;
+    }
+    *loss = L;
+}
+
+__global__ void adj_sum_kernel(const double *acc, int n, double *out)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double s = 0.0;
+    for (int i = 0; i < n; i++) s += acc[i];
+    *out = s;
+}
+
+} // namespace
+
+extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double *loss, double *grad_tin,
+                               double *grad_tau_g)
+{
+    if (!c || !spec || !loss || !grad_tau_g) return bgk_internal_fail(BGK_ERR_ARG, "null argument");
+    if (c->opt.precision != BGK_PREC_F64 || !c->opt.smooth)
+        return bgk_internal_fail(BGK_ERR_UNSUPPORTED, "the adjoint differentiates the smooth FP64 form: create the "
+                                                      "context with precision BGK_PREC_F64 and smooth = 1");
+    const int N = spec->nsteps;
+    if (N < 1) return bgk_internal_fail(BGK_ERR_ARG, "nsteps must be >= 1");
+    if (spec->nprobes < 1 || !spec->probe_i || !spec->probe_j || !spec->phi_target)
+        return bgk_internal_fail(BGK_ERR_ARG, "at least one probe is needed");
+    for (int p = 0; p < spec->nprobes; p++)
+        if (spec->probe_i[p] < 1 || spec->probe_i[p] > c->Nx || spec->probe_j[p] < 1 || spec->probe_j[p] > c->Ny)
+            return bgk_internal_fail(BGK_ERR_ARG, "probe outside 1..Nx x 1..Ny");
+    int K = spec->checkpoint_every;
+    if (K <= 0) K = (int)std::ceil(std::sqrt((double)N));
+    if (K > N) K = N;
+    int rc = bgk_internal_prepare_fused(c);
+    if (rc) return rc;
+
+    cudaStream_t st = c->stream;
+    const long long pl = c->plane;
+    const int Ny = c->Ny;
+    /* one stored state: f (9 planes), g (9), phi (1), T column (Ny, padded) */
+    const long long tc_pad = ((long long)Ny + 31) / 32 * 32;
+    const size_t state_elems = (size_t)(19 * pl + tc_pad);
+    const int nsnap = (N + K - 1) / K;    /* snapshots of S(0), S(K), ...    */
+    std::vector<void *> allocs;
+    auto dmalloc = [&](size_t bytes) -> double * {
+        void *p = nullptr;
+        if (cudaMalloc(&p, bytes) != cudaSuccess) { (void)cudaGetLastError(); return nullptr; }
+        allocs.push_back(p);
+        return (double *)p;
+    };
+    auto cleanup = [&]() { for (void *p : allocs) cudaFree(p); };
+    double *snaps = dmalloc((size_t)nsnap * state_elems * sizeof(double));
+    double *seg = dmalloc((size_t)(K + 1) * state_elems * sizeof(double));
+    double *pi[2] = {dmalloc((size_t)NPI * pl * sizeof(double)), dmalloc((size_t)NPI * pl * sizeof(double))};
+    dim3 blk(AB_X, AB_Y), grd((c->Nx + AB_X - 1) / AB_X, (Ny + AB_Y - 1) / AB_Y);
+    const int nblk = grd.x * grd.y;
+    double *omg_acc = dmalloc((size_t)nblk * sizeof(double));
+    double *dgW = dmalloc(3 * (size_t)Ny * sizeof(double));
+    double *gtin = dmalloc((size_t)Ny * sizeof(double));
+    double *scal = dmalloc(4 * sizeof(double));
+    int *dpi = (int *)dmalloc((size_t)spec->nprobes * sizeof(int) + 16);
+    int *dpj = (int *)dmalloc((size_t)spec->nprobes * sizeof(int) + 16);
+    double *dtg = dmalloc((size_t)spec->nprobes * sizeof(double));
+    if (!snaps || !seg || !pi[0] || !pi[1] || !omg_acc || !dgW || !gtin || !scal || !dpi || !dpj || !dtg) {
+        cleanup();
+        return bgk_internal_fail(BGK_ERR_OOM, "adjoint workspace allocation failed");
+    }
+#define ACK(call)                                                                   \
+    do {                                                                            \
+        cudaError_t e_ = (call);                                                    \
+        if (e_ != cudaSuccess) {                                                    \
+            cleanup();                                                              \
+            return bgk_internal_fail(BGK_ERR_CUDA, cudaGetErrorString(e_));         \
+        }                                                                           \
+    } while (0)
+    auto copy_state_in = [&](double *dst, int buf) -> cudaError_t {
+        cudaError_t e;
+        if ((e = cudaMemcpyAsync(dst, c->fbuf[buf], 9 * pl * sizeof(double), cudaMemcpyDeviceToDevice, st))) return e;
+        if ((e = cudaMemcpyAsync(dst + 9 * pl, c->gbuf[buf], 9 * pl * sizeof(double), cudaMemcpyDeviceToDevice, st)))
+            return e;
+        if ((e = cudaMemcpyAsync(dst + 18 * pl, c->phibuf[buf], pl * sizeof(double), cudaMemcpyDeviceToDevice, st)))
+            return e;
+        return cudaMemcpyAsync(dst + 19 * pl, c->tcol[buf], Ny * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    };
+
+    ACK(cudaMemcpyAsync(dpi, spec->probe_i, spec->nprobes * sizeof(int), cudaMemcpyHostToDevice, st));
+    ACK(cudaMemcpyAsync(dpj, spec->probe_j, spec->nprobes * sizeof(int), cudaMemcpyHostToDevice, st));
+    ACK(cudaMemcpyAsync(dtg, spec->phi_target, spec->nprobes * sizeof(double), cudaMemcpyHostToDevice, st));
+    adj_dgw_kernel<<<(Ny + 127) / 128, 128, 0, st>>>(c->c, c->mu, c->mv, dgW);
+    ACK(cudaGetLastError());
+
+    /* forward pass on the context, snapshots every K steps */
+    ACK(copy_state_in(snaps, c->cur));
+    for (int n0 = 0; n0 < N; n0 += K) {
+        const int len = (n0 + K < N) ? K : N - n0;
+        rc = bgk_step(c, len);
+        if (rc) { cleanup(); return rc; }
+        if (n0 + len < N) ACK(copy_state_in(snaps + (size_t)((n0 + len) / K) * state_elems, c->cur));
+    }
+    /* loss and seed */
+    ACK(cudaMemsetAsync(pi[0], 0, (size_t)NPI * pl * sizeof(double), st));
+    ACK(cudaMemsetAsync(omg_acc, 0, (size_t)nblk * sizeof(double), st));
+    ACK(cudaMemsetAsync(gtin, 0, (size_t)Ny * sizeof(double), st));
+    adj_seed_kernel<<<1, 32, 0, st>>>((const double *)c->phibuf[c->cur], pl, c->P, spec->nprobes, dpi, dpj, dtg,
+                                      pi[0] + 20 * pl, scal);
+    ACK(cudaGetLastError());
+
+    /* reverse sweep, one segment at a time */
+    int pin = 0;
+    for (int sgi = nsnap - 1; sgi >= 0; sgi--) {
+        const int n0 = sgi * K;
+        const int n1 = (n0 + K < N) ? n0 + K : N;
+        /* states S(n0) .. S(n1-1) into seg[0 .. n1-n0-1] */
+        ACK(cudaMemcpyAsync(seg, snaps + (size_t)sgi * state_elems, state_elems * sizeof(double),
+                            cudaMemcpyDeviceToDevice, st));
+        for (int n = n0 + 1; n < n1; n++) {
+            double *a = seg + (size_t)(n - 1 - n0) * state_elems;
+            double *b = seg + (size_t)(n - n0) * state_elems;
+            ACK(bgk::launch_fused_f64_ptrs(c, a, a + 9 * pl, a + 18 * pl, a + 19 * pl, b, b + 9 * pl, b + 18 * pl,
+                                           b + 19 * pl));
+        }
+        for (int n = n1; n > n0; n--) {
+            const double *S0 = seg + (size_t)(n - 1 - n0) * state_elems;
+            AdjPtrs a{};
+            a.f = S0; a.g = S0 + 9 * pl; a.phi = S0 + 18 * pl; a.tcol = S0 + 19 * pl;
+            a.pin = pi[pin]; a.pout = pi[pin ^ 1];
+            a.gW = c->gW; a.pE = c->pE; a.phiW = c->phiW; a.phiE = c->phiE; a.corner = c->corner;
+            a.omg_acc = omg_acc;
+            a.plane = pl; a.P = c->P;
+            a.tanh_mode = c->opt.tanh_mode;
+            adj_step_kernel<<<grd, blk, 0, st>>>(a, c->c);
+            ACK(cudaGetLastError());
+            adj_tin_kernel<<<1, 1024, 0, st>>>(pi[pin ^ 1], pl, c->P, Ny, dgW, gtin);
+            ACK(cudaGetLastError());
+            pin ^= 1;
+        }
+    }
+    adj_sum_kernel<<<1, 32, 0, st>>>(omg_acc, nblk, scal + 1);
+    ACK(cudaGetLastError());
+    double host[2];
+    ACK(cudaMemcpyAsync(host, scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (grad_tin) ACK(cudaMemcpyAsync(grad_tin, gtin, (size_t)Ny * sizeof(double), cudaMemcpyDeviceToHost, st));
+    ACK(cudaStreamSynchronize(st));
+    *loss = host[0];
+    /* omega_g = 1/tau_g */
+    const double tau_g = c->p.tau_g;
+    *grad_tau_g = host[1] * (-1.0 / (tau_g * tau_g));
+    cleanup();
+#undef ACK
+    return BGK_OK;
+}

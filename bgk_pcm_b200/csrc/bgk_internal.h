@@ -144,11 +144,17 @@ cudaError_t launch_staged_to_compact(bgk_ctx *c);
 cudaError_t launch_ref_to_compact(bgk_ctx *c, int field, const double *ref);
 cudaError_t launch_compact_to_ref(bgk_ctx *c, int field, double *ref, int which);
 cudaError_t launch_field_sums(bgk_ctx *c);   /* -> c->red[0..3] */
+cudaError_t launch_fused_f64_ptrs(bgk_ctx *c, const double *fin, const double *gin, const double *phin,
+                                  const double *tcin, double *fout, double *gout, double *phout, double *tcout);
 
 /* kernels_fast.cu (FMA allowed): FP64-FMA, FP32 and FP16 forms */
 cudaError_t launch_fused_fast(bgk_ctx *c, bool moments);
 cudaError_t launch_init_lowp(bgk_ctx *c);
 
 } // namespace bgk
+
+/* capi.cu helpers shared with adjoint.cu */
+int bgk_internal_fail(int code, const char *msg);
+int bgk_internal_prepare_fused(bgk_ctx *c);   /* device, fused state, BC arrays */
 
 #endif

@@ -314,6 +314,22 @@ int field_source(bgk_ctx *c, int field, const double **src)
 
 } // namespace
 
+int bgk_internal_fail(int code, const char *msg) { return fail(code, "%s", msg); }
+
+int bgk_internal_prepare_fused(bgk_ctx *c)
+{
+    if (!all_bc4(c->p))
+        return fail(BGK_ERR_UNSUPPORTED, "the fused step implements the no-slip code 4 on every wall");
+    int rc = set_device(c);
+    if (rc) return rc;
+    if ((rc = ensure_fused(c))) return rc;
+    if (c->bc_dirty) {
+        CK(bgk::launch_bc_prep(c), "bc_prep");
+        c->bc_dirty = false;
+    }
+    return BGK_OK;
+}
+
 extern "C" {
 
 const char *bgk_last_error(void) { return g_err; }

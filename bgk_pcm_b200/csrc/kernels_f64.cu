@@ -619,6 +619,22 @@ cudaError_t launch_fused_f64(bgk_ctx *c, bool moments)
     return launch_fused_f64_variant(c, grd, s, H, moments);
 }
 
+/* One fused step between explicit state buffers (no moments written):
+ * used by the adjoint to recompute checkpointed segments. */
+cudaError_t launch_fused_f64_ptrs(bgk_ctx *c, const double *fin, const double *gin, const double *phin,
+                                  const double *tcin, double *fout, double *gout, double *phout, double *tcout)
+{
+    StepPtrs<double> s{};
+    s.fin = fin; s.gin = gin; s.fout = fout; s.gout = gout;
+    s.phin = phin; s.phout = phout; s.tcin = tcin; s.tcout = tcout;
+    s.gW = c->gW; s.pE = c->pE; s.phiW = c->phiW; s.phiE = c->phiE;
+    s.mrho = c->mrho; s.mT = c->mT; s.mu = c->mu; s.mv = c->mv; s.mphi = c->mphi;
+    s.plane = c->plane; s.P = c->P; s.NX2 = c->NX2;
+    const int H = strip_height(c);
+    dim3 grd((c->Nx + FUSED_BX - 1) / FUSED_BX, (c->Ny + H - 1) / H);
+    return launch_fused_f64_variant(c, grd, s, H, false);
+}
+
 cudaError_t launch_staged(bgk_ctx *c, int stage)
 {
     Staged s = staged_of(c);

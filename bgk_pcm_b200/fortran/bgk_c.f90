@@ -21,6 +21,11 @@ module bgk_c
      integer(c_int) :: westBC, eastBC, northBC, southBC
   end type bgk_params
 
+  type, bind(c) :: bgk_adjoint_spec
+     integer(c_int) :: nsteps, checkpoint_every, nprobes
+     type(c_ptr) :: probe_i, probe_j, phi_target
+  end type bgk_adjoint_spec
+
   type, bind(c) :: bgk_options
      integer(c_int) :: precision, tanh_mode, fma, device, smooth
   end type bgk_options
@@ -157,6 +162,20 @@ module bgk_c
        import :: c_int, c_ptr, c_char
        type(c_ptr), value :: ctx
        character(kind=c_char), dimension(*), intent(in) :: path
+       integer(c_int) :: rc
+     end function
+     function bgk_adjoint_run(ctx, spec, loss, grad_tin, grad_tau_g) bind(c, name="bgk_adjoint_run") result(rc)
+       import :: c_int, c_ptr, c_double, bgk_adjoint_spec
+       type(c_ptr), value :: ctx
+       type(bgk_adjoint_spec), intent(in) :: spec
+       real(c_double), intent(out) :: loss, grad_tau_g
+       real(c_double), dimension(*), intent(out) :: grad_tin
+       integer(c_int) :: rc
+     end function
+     function bgk_get_stream(ctx, stream) bind(c, name="bgk_get_stream") result(rc)
+       import :: c_int, c_ptr
+       type(c_ptr), value :: ctx
+       type(c_ptr), intent(out) :: stream
        integer(c_int) :: rc
      end function
      function bgk_last_error() bind(c, name="bgk_last_error") result(msg)

@@ -1,0 +1,87 @@
+"""The differentiation workload (512x512 cavity, Ra 1e5, 2000 steps): probes,
+seeded parameters and the finite-difference check of the adjoint gradient.
+
+Loss L = sum over 64 probe nodes of (phi_final - phi_target)^2, phi_target
+from a run with a seeded perturbation of the hot-wall temperatures.
+Parameters: Tin_j = T0 + dT * 0.05 * N(0,1) per row (the hot wall at 1 +
+0.05 N(0,1) in units of the temperature span dT = T0 - T_in_sol) and tau_g.
+Probes sit in the band i in [Nx/40, Nx/40 + 32] that the melting front
+reaches within the run.
+"""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+
+from . import inputs
+from .solver import Solver
+
+
+def setup(Nx=512, Ny=512, steps=2000, Ra=1e5, seed=0, nprobes=64, **overrides):
+    p = inputs.workload_params(Nx=Nx, Ny=Ny, iter=steps, Ra=Ra)
+    p.update(overrides)
+    rng = np.random.default_rng(seed)
+    dT = p["T0"] - p["T_in_sol"]
+    tin = p["T0"] + dT * 0.05 * rng.standard_normal(Ny)
+    tin_target = p["T0"] + dT * 0.05 * rng.standard_normal(Ny)
+    i0 = Nx // 40
+    pi = i0 + rng.integers(0, min(33, Nx - i0), nprobes) if Nx - i0 > 1 else np.full(nprobes, 1)
+    pi = np.clip(pi, 1, Nx)
+    pj = rng.integers(1, Ny + 1, nprobes)
+    return p, tin, tin_target, pi.astype(np.int32), pj.astype(np.int32)
+
+
+def forward_phi(p, tin, steps, pi, pj, tau_g=None):
+    q = dict(p)
+    if tau_g is not None:
+        q["tau_g"] = tau_g
+    s = Solver(q, smooth=True)
+    s.initialization()
+    s.set_tin(tin)
+    s.step(steps)
+    phi = s.field("phi")
+    s.close()
+    return phi[pj, pi]
+
+
+def loss_of(p, tin, steps, pi, pj, target, tau_g=None):
+    r = forward_phi(p, tin, steps, pi, pj, tau_g) - target
+    return float(np.sum(r * r))
+
+
+def adjoint(p, tin, steps, pi, pj, target, checkpoint_every=45):
+    s = Solver(p, smooth=True)
+    s.initialization()
+    s.set_tin(tin)
+    out = s.adjoint(steps, pi, pj, target, checkpoint_every)
+    s.close()
+    return out
+
+
+def fd_check(p, tin, steps, pi, pj, target, grad_tin, grad_tau, ndir=16, h=1e-6, seed=1):
+    """Central differences along random unit directions in (Tin, tau_g)."""
+    rng = np.random.default_rng(seed)
+    rows = []
+    for _ in range(ndir):
+        v = rng.standard_normal(p["Ny"] + 1)
+        v /= np.linalg.norm(v)
+        vt, vtau = v[:-1], v[-1]
+        lp = loss_of(p, tin + h * vt, steps, pi, pj, target, p["tau_g"] + h * vtau)
+        lm = loss_of(p, tin - h * vt, steps, pi, pj, target, p["tau_g"] - h * vtau)
+        fd = (lp - lm) / (2 * h)
+        ad = float(grad_tin @ vt + grad_tau * vtau)
+        rows.append((fd, ad, abs(fd - ad) / max(abs(ad), 1e-300)))
+    return rows
+
+
+def cost_ratio(p, tin, steps, pi, pj, target, checkpoint_every=45, repeats=3):
+    import torch
+    fw, ad = [], []
+    for _ in range(repeats):
+        s = Solver(p, smooth=True); s.initialization(); s.set_tin(tin); s.sync()
+        t0 = time.perf_counter(); s.step(steps); s.sync(); fw.append(time.perf_counter() - t0); s.close()
+        s = Solver(p, smooth=True); s.initialization(); s.set_tin(tin); s.sync()
+        t0 = time.perf_counter(); s.adjoint(steps, pi, pj, target, checkpoint_every); ad.append(time.perf_counter() - t0)
+        s.close()
+    return min(ad) / min(fw), min(fw), min(ad)

@@ -158,6 +158,25 @@ class Solver:
         capi.check(self._lib.bgk_get_stream(self._h, ctypes.byref(v)))
         return v.value or 0
 
+    def adjoint(self, nsteps: int, probe_i, probe_j, phi_target, checkpoint_every: int = 0):
+        """Loss sum_p (phi(i_p,j_p) - target_p)^2 after nsteps steps from the
+        current state, with dL/dTin (per row, length Ny) and dL/dtau_g.
+        Requires a context created with smooth=True."""
+        pi = np.ascontiguousarray(probe_i, dtype=np.int32)
+        pj = np.ascontiguousarray(probe_j, dtype=np.int32)
+        tg = np.ascontiguousarray(phi_target, dtype=np.float64)
+        if not (pi.size == pj.size == tg.size):
+            raise ValueError("probe_i, probe_j and phi_target must have the same length")
+        spec = capi.AdjointSpec(int(nsteps), int(checkpoint_every), int(pi.size),
+                                pi.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                pj.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dptr(tg))
+        loss = ctypes.c_double()
+        gtau = ctypes.c_double()
+        gtin = np.zeros(self.Ny, dtype=np.float64)
+        capi.check(self._lib.bgk_adjoint_run(self._h, ctypes.byref(spec), ctypes.byref(loss), _dptr(gtin),
+                                             ctypes.byref(gtau)))
+        return loss.value, gtin, gtau.value
+
     def save(self, path) -> None:
         capi.check(self._lib.bgk_save(self._h, str(Path(path)).encode()))
 

@@ -177,6 +177,31 @@ int bgk_sync(bgk_ctx *ctx);
  * counterpart (the reference has no device streams). */
 int bgk_get_stream(bgk_ctx *ctx, void **stream);
 
+/* ----------------------------------------------------- differentiation form */
+/* Loss L = sum_p (phi(i_p, j_p) - phi_target_p)^2 on the state reached after
+ * nsteps fused steps from the current state. */
+typedef struct bgk_adjoint_spec {
+    int nsteps;                /* forward steps from the current state           */
+    int checkpoint_every;      /* snapshot interval K (<= 0: ceil(sqrt(nsteps)))  */
+    int nprobes;
+    const int *probe_i;        /* reference indices, 1..Nx                       */
+    const int *probe_j;        /* 1..Ny                                          */
+    const double *phi_target;  /* nprobes values                                 */
+} bgk_adjoint_spec;
+
+/* L and its gradient with respect to the per-row hot-wall temperatures
+ * (grad_tin[j-1] = dL/dTin_j, the Tin of STEP_7/BC_g.f90:13-16 generalised
+ * per row by bgk_set_tin) and to the thermal relaxation time tau_g
+ * (STEP_7/setup.f90:103), by a hand-written reverse of the fused step run
+ * backward in time with checkpoint-and-recompute: snapshots every K steps,
+ * each K-step segment recomputed forward before it is reversed.  No
+ * reference counterpart (the reference has no derivatives).  Requires an FP64
+ * context created with opt.smooth = 1 (the differentiable form).  The
+ * context is left at the final state, exactly as bgk_step(ctx, nsteps)
+ * leaves it.  grad_tin may be NULL. */
+int bgk_adjoint_run(bgk_ctx *ctx, const bgk_adjoint_spec *spec, double *loss,
+                    double *grad_tin, double *grad_tau_g);
+
 /* Complete binary snapshot (populations, phi, frozen boundary values, it)
  * -- unlike the reference's text dump (STEP_7/dump_out.f90:5-18), which omits
  * phi and phi_prec.  A snapshot restores into a context of the same size and

@@ -71,6 +71,11 @@ def load() -> ctypes.CDLL:
     lib.orc_main.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
     lib.orc_portable_tanh.restype = ctypes.c_double
     lib.orc_portable_tanh.argtypes = [ctypes.c_double]
+    dp = ctypes.POINTER(ctypes.c_double)
+    ip = ctypes.POINTER(ctypes.c_int)
+    lib.orc_tangent_loss.argtypes = [ctypes.POINTER(OrcParams), dp, dp, ctypes.c_double, ctypes.c_int,
+                                     ctypes.c_int, ip, ip, dp, dp, dp, dp]
+    lib.orc_tangent_plain.argtypes = [ctypes.POINTER(OrcParams), dp, ctypes.c_int, dp, dp]
     _lib = lib
     return lib
 
@@ -155,3 +160,43 @@ def run_main(workdir, threads: int = 0, tanh_mode: int = 0) -> None:
     r = subprocess.run([str(MAIN), str(workdir), str(threads), str(tanh_mode)], capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(r.stderr)
+
+
+def _params(d: dict) -> OrcParams:
+    p = OrcParams()
+    for n, _ in OrcParams._fields_:
+        setattr(p, n, d[n])
+    return p
+
+
+def tangent_loss(params: dict, tin, dtin, dtau_g: float, nsteps: int, pi, pj, target):
+    """Loss and its directional derivative along (dtin, dtau_g), by forward
+    mode (dual numbers) through the reference's step (smooth form)."""
+    dpt = ctypes.POINTER(ctypes.c_double)
+    tin = np.ascontiguousarray(tin, dtype=np.float64)
+    dtin = np.ascontiguousarray(dtin, dtype=np.float64)
+    pi = np.ascontiguousarray(pi, dtype=np.int32)
+    pj = np.ascontiguousarray(pj, dtype=np.int32)
+    target = np.ascontiguousarray(target, dtype=np.float64)
+    loss = ctypes.c_double()
+    dloss = ctypes.c_double()
+    rc = load().orc_tangent_loss(ctypes.byref(_params(params)), tin.ctypes.data_as(dpt), dtin.ctypes.data_as(dpt),
+                                 float(dtau_g), int(nsteps), int(pi.size),
+                                 pi.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                 pj.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), target.ctypes.data_as(dpt),
+                                 ctypes.byref(loss), ctypes.byref(dloss), None)
+    if rc:
+        raise ValueError("tangent oracle supports the no-slip cavity with Re = 0 only")
+    return loss.value, dloss.value
+
+
+def tangent_plain(params: dict, tin, nsteps: int):
+    """phi and T after nsteps of the templated restatement in plain double."""
+    dpt = ctypes.POINTER(ctypes.c_double)
+    tin = np.ascontiguousarray(tin, dtype=np.float64)
+    shape = (params["Ny"] + 2, params["Nx"] + 2)
+    phi = np.empty(shape)
+    T = np.empty(shape)
+    load().orc_tangent_plain(ctypes.byref(_params(params)), tin.ctypes.data_as(dpt), int(nsteps),
+                             phi.ctypes.data_as(dpt), T.ctypes.data_as(dpt))
+    return phi, T

@@ -1,0 +1,80 @@
+"""The differentiation form: the hand-written adjoint of the fused step
+against central finite differences of the (smooth) FP64 forward."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+# solid just below T_crit so that the small cavities respond within a few steps
+SENSITIVE = dict(T_in_sol=271.0)
+
+
+@pytest.mark.parametrize("Nx,Ny,steps,K", [(24, 16, 6, 4), (40, 33, 30, 7), (13, 1, 5, 2)])
+def test_adjoint_small_fd(lib, Nx, Ny, steps, K):
+    from bgk_pcm_b200 import gradcheck as gc
+    p, tin, tin_t, pi, pj = gc.setup(Nx=Nx, Ny=Ny, steps=steps, nprobes=12, **SENSITIVE)
+    pi = np.clip(pi, 1, Nx)
+    target = gc.forward_phi(p, tin_t, steps, pi, pj)
+    loss, g, gtau = gc.adjoint(p, tin, steps, pi, pj, target, checkpoint_every=K)
+    assert abs(loss - gc.loss_of(p, tin, steps, pi, pj, target)) <= 1e-12 * max(loss, 1e-300)
+    rows = gc.fd_check(p, tin, steps, pi, pj, target, g, gtau, ndir=6, h=1e-5)
+    for fd, ad, rel in rows:
+        assert rel < 1e-5 or abs(fd - ad) < 1e-12, rows
+
+
+def test_adjoint_matches_tangent_oracle(oracle_mod, lib):
+    """<grad L, v> from the adjoint equals the forward-mode derivative of the
+    CPU restatement (dual numbers) along random directions v."""
+    from bgk_pcm_b200 import gradcheck as gc
+    p, tin, tin_t, pi, pj = gc.setup(Nx=20, Ny=14, steps=40, nprobes=8, **SENSITIVE)
+    pi = np.clip(pi, 1, 6)
+    target = gc.forward_phi(p, tin_t, 40, pi, pj)
+    loss, g, gtau = gc.adjoint(p, tin, 40, pi, pj, target, checkpoint_every=7)
+    rng = np.random.default_rng(5)
+    for _ in range(4):
+        v = rng.standard_normal(p["Ny"] + 1)
+        Lt, dLt = oracle_mod.tangent_loss(p, tin, v[:-1], v[-1], 40, pi, pj, target)
+        assert abs(Lt - loss) <= 1e-10 * abs(loss)
+        ad = float(g @ v[:-1] + gtau * v[-1])
+        assert abs(ad - dLt) <= 1e-8 * abs(dLt), (ad, dLt)
+
+
+def test_adjoint_checkpoint_interval_invariant(lib):
+    from bgk_pcm_b200 import gradcheck as gc
+    p, tin, tin_t, pi, pj = gc.setup(Nx=32, Ny=24, steps=20, nprobes=10, **SENSITIVE)
+    target = gc.forward_phi(p, tin_t, 20, pi, pj)
+    a = gc.adjoint(p, tin, 20, pi, pj, target, checkpoint_every=20)
+    b = gc.adjoint(p, tin, 20, pi, pj, target, checkpoint_every=3)
+    assert a[0] == b[0]
+    np.testing.assert_allclose(b[1], a[1], rtol=1e-12, atol=1e-300)
+    assert abs(a[2] - b[2]) <= 1e-12 * abs(a[2])
+
+
+def test_adjoint_requires_smooth(lib):
+    from bgk_pcm_b200 import BGKError, Solver, inputs
+    p = inputs.workload_params(Nx=16, Ny=16, iter=10, Ra=1e5)
+    s = Solver(p)
+    s.initialization()
+    with pytest.raises(BGKError, match="UNSUPPORTED"):
+        s.adjoint(3, [2], [2], [0.0])
+
+
+@pytest.mark.slow
+def test_adjoint_config4_fd_16_directions(lib):
+    """512x512, Ra 1e5, 2000 steps, 64 probes, checkpoints every 45 steps:
+    relative error <= 1e-5 against central differences (h = 1e-6) on 16
+    random directions, and the gradient costs <= 4 forward solves."""
+    from bgk_pcm_b200 import gradcheck as gc
+    p, tin, tin_t, pi, pj = gc.setup()
+    target = gc.forward_phi(p, tin_t, 2000, pi, pj)
+    loss, g, gtau = gc.adjoint(p, tin, 2000, pi, pj, target, checkpoint_every=45)
+    rows = gc.fd_check(p, tin, 2000, pi, pj, target, g, gtau, ndir=16, h=1e-6)
+    worst = max(r[2] for r in rows)
+    print("adjoint config4: loss", loss, "worst rel err", worst)
+    assert worst <= 1e-5, rows
+    ratio, tf, ta = gc.cost_ratio(p, tin, 2000, pi, pj, target)
+    print(f"adjoint/forward cost {ratio:.2f} (forward {tf*1e3:.1f} ms, adjoint {ta*1e3:.1f} ms)")
+    assert ratio <= 4.0
