@@ -81,12 +81,16 @@ __device__ __forceinline__ void eq_poly_grad(double u, double v, double *du, dou
 
 /* Vector-Jacobian product of one node update (smooth form).
  * in : pulled f, g; selector sums kp, km; phi_prec p0; output adjoints
- *      Fo_b (f post-collision), Go_b (g post-collision), phn_b (new phi),
- *      Tm_b (moments T written for the east boundary).
+ *      Fo_b (f post-collision), Go_b (g post-collision), Tm_b (moments T
+ *      written for the east boundary) and the adjoint of the new phi in
+ *      gathered form: phi_b = d0 + aplus'(phn) * skp + aminus'(phn) * skm,
+ *      where the selector-term derivatives are taken at the new value phn
+ *      (the value the next step's stencils read).
  * out: f_b, g_b (pulled), kp_b, km_b, p0_b, omg_b (d/d omega_g). */
 __device__ void node_vjp(const Consts &c, int tanh_mode, const double *f, const double *g, double kp, double km,
-                         double p0, const double *Fo_b, const double *Go_b, double phn_b, double Tm_b, double *f_b,
-                         double *g_b, double &kp_b, double &km_b, double &p0_b, double &omg_b)
+                         double p0, const double *Fo_b, const double *Go_b, double d0, double skp, double skm,
+                         double Tm_b, double *f_b, double *g_b, double &kp_b, double &km_b, double &p0_b,
+                         double &omg_b)
 {
     const double m = c.m_cs2, q = c.q_cs2;
     /* ---- forward recompute ---- */
@@ -102,6 +106,7 @@ __device__ void node_vjp(const Consts &c, int tanh_mode, const double *f, const 
     const double rp = 0.5 * (1.0 + th), rm = 0.5 * (1.0 - th);
     const double KP = (kp / 8.0) * rp, KM = (km / 8.0) * rm;
     const double phn = p0 + (c.f_plus * KP * (1.0 - p0) - c.f_minus * KM * (1.0 + p0));
+    const double phn_b = d0 + 0.5 * (1.0 + phn) * skp - 0.5 * (1.0 - phn) * skm;
     const double Tf = T - c.dts * (phn - p0) / 2.0;
     const double gb = c.grav * c.beta;
     const double onep = 1.0 + phn / 2.0;
@@ -252,8 +257,8 @@ adj_step_kernel(AdjPtrs s, Consts c)
                 if (dy == 1 && y == Ny - 1) { skp += PI(s, 18, xd, Ny - 1); skm += PI(s, 19, xd, Ny - 1); }
             }
         }
-        const double ph = s.phi[cc];
-        const double lphi = PI(s, 20, x, y) + 0.5 * (1.0 + ph) * skp - 0.5 * (1.0 - ph) * skm;
+        const double ph = s.phi[cc];        /* phi_prec of step n */
+        const double d0 = PI(s, 20, x, y);
         /* T(Nx, y) written by this (east) node: read by the east pulls of
          * pops 3 (same row), 6 (row y+1, or row 0 itself) and 7 (row y-1, or
          * row Ny-1 itself) of the next step */
@@ -312,7 +317,7 @@ adj_step_kernel(AdjPtrs s, Consts c)
 
         /* 3. vector-Jacobian product -> Pi(n) */
         double fb[9], gbv[9], kpb, kmb, p0b;
-        node_vjp(c, s.tanh_mode, f, g, kp, km, ph, lf, lg, lphi, lT, fb, gbv, kpb, kmb, p0b, omg_b);
+        node_vjp(c, s.tanh_mode, f, g, kp, km, ph, lf, lg, d0, skp, skm, lT, fb, gbv, kpb, kmb, p0b, omg_b);
 #pragma unroll
         for (int k = 0; k < 9; k++) {
             s.pout[k * pl + cc] = fb[k];

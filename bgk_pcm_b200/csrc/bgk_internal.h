@@ -100,8 +100,12 @@ struct bgk_ctx {
     size_t phisz;          /* bytes per stored phi element (4 or 8)          */
     int it;
 
-    /* fused state */
+    /* fused state (each buffer has a 256-byte guard on both sides: the
+     * shared-memory pipeline copies row segments that start 16 bytes before a
+     * band and may end 16 bytes after a row) */
     void *fbuf[2], *gbuf[2], *phibuf[2];
+    void *raw[6];          /* allocation bases of fbuf, gbuf, phibuf        */
+    int *errflag;          /* device: nonzero after a bounded wait gave up   */
     int cur;
     double *tcol[2];
     double *gW, *pE, *phiW, *phiE;
@@ -129,6 +133,10 @@ struct bgk_ctx {
      * L2 prefetch distance in rows (0 = off); BGK_STRIP_H / BGK_PREFETCH_ROWS
      * override the defaults at bgk_create */
     int tune_H, tune_pf;
+    /* kernel choice: 1 = shared-memory pipeline (default), 0 = register
+     * pulls; pipeline depth and CTAs per SM (BGK_PIPE, BGK_PIPE_D,
+     * BGK_PIPE_CTAS) */
+    int tune_pipe, tune_D, tune_ctas, nsm;
 };
 
 namespace bgk {

@@ -410,23 +410,40 @@ int bgk_create(const bgk_params *pp, const bgk_options *opt, bgk_ctx **out)
     c->bc_dirty = true;
     c->tune_H = 0;
     c->tune_pf = 2;
+    c->tune_pipe = 1;
+    c->tune_D = 0;
+    c->tune_ctas = 0;
     if (const char *v = getenv("BGK_STRIP_H")) c->tune_H = atoi(v);
     if (const char *v = getenv("BGK_PREFETCH_ROWS")) c->tune_pf = atoi(v);
+    if (const char *v = getenv("BGK_PIPE")) c->tune_pipe = atoi(v);
+    if (const char *v = getenv("BGK_PIPE_D")) c->tune_D = atoi(v);
+    if (const char *v = getenv("BGK_PIPE_CTAS")) c->tune_ctas = atoi(v);
+    {
+        cudaDeviceProp pr;
+        c->nsm = (cudaGetDeviceProperties(&pr, dev) == cudaSuccess) ? pr.multiProcessorCount : 148;
+    }
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { delete c; return cuda_fail(e, "cudaStreamCreate"); }
 
-    /* 9 planes per distribution plus one row of guard on each side */
-    const size_t popbytes = (size_t)(9 * c->plane + 2 * c->P) * c->esz;
-    const size_t phibytes = (size_t)(c->plane + 2 * c->P) * c->phisz;
+    /* 9 planes per distribution, then slack for the pipeline's last row
+     * segment (a band of 128 columns + 16 bytes may run past the last row) */
+    const size_t popbytes = (size_t)(9 * c->plane + 2 * c->P + 256) * c->esz;
+    const size_t phibytes = (size_t)(c->plane + 2 * c->P + 256) * c->phisz;
+    const size_t guard = 256;
     for (int b = 0; b < 2; b++) {
-        DA(c->fbuf[b], popbytes, "f populations");
-        DA(c->gbuf[b], popbytes, "g populations");
-        DA(c->phibuf[b], phibytes, "phi");
-        CK(cudaMemsetAsync(c->fbuf[b], 0, popbytes, c->stream), "memset");
-        CK(cudaMemsetAsync(c->gbuf[b], 0, popbytes, c->stream), "memset");
-        CK(cudaMemsetAsync(c->phibuf[b], 0, phibytes, c->stream), "memset");
+        DA(c->raw[b], popbytes + 2 * guard, "f populations");
+        DA(c->raw[2 + b], popbytes + 2 * guard, "g populations");
+        DA(c->raw[4 + b], phibytes + 2 * guard, "phi");
+        CK(cudaMemsetAsync(c->raw[b], 0, popbytes + 2 * guard, c->stream), "memset");
+        CK(cudaMemsetAsync(c->raw[2 + b], 0, popbytes + 2 * guard, c->stream), "memset");
+        CK(cudaMemsetAsync(c->raw[4 + b], 0, phibytes + 2 * guard, c->stream), "memset");
+        c->fbuf[b] = (char *)c->raw[b] + guard;
+        c->gbuf[b] = (char *)c->raw[2 + b] + guard;
+        c->phibuf[b] = (char *)c->raw[4 + b] + guard;
         DA(c->tcol[b], (size_t)c->Ny * sizeof(double), "T column");
     }
+    DA(c->errflag, sizeof(int), "error flag");
+    CK(cudaMemsetAsync(c->errflag, 0, sizeof(int), c->stream), "memset");
     DA(c->gW, 3 * (size_t)c->Ny * sizeof(double), "west g");
     DA(c->pE, 3 * (size_t)c->Ny * sizeof(double), "east poly");
     DA(c->phiW, (size_t)c->Ny * sizeof(double), "phi west");
@@ -453,7 +470,7 @@ int bgk_destroy(bgk_ctx *c)
     if (!c) return BGK_OK;
     cudaSetDevice(c->dev);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    void *ptrs[] = {c->fbuf[0], c->fbuf[1], c->gbuf[0], c->gbuf[1], c->phibuf[0], c->phibuf[1],
+    void *ptrs[] = {c->raw[0], c->raw[1], c->raw[2], c->raw[3], c->raw[4], c->raw[5], c->errflag,
                     c->tcol[0], c->tcol[1], c->gW, c->pE, c->phiW, c->phiE, c->tin_rows,
                     c->mrho, c->mT, c->mu, c->mv, c->mphi, c->sphip, c->srho2, c->sT2, c->su2, c->sv2,
                     c->scratch, c->red, c->corner};
@@ -671,6 +688,12 @@ int bgk_sync(bgk_ctx *c)
     int rc = set_device(c);
     if (rc) return rc;
     CK(cudaStreamSynchronize(c->stream), "sync");
+    int flag = 0;
+    CK(cudaMemcpy(&flag, c->errflag, sizeof(int), cudaMemcpyDeviceToHost), "error flag");
+    if (flag) {
+        cudaMemset(c->errflag, 0, sizeof(int));
+        return fail(BGK_ERR_CUDA, "a bounded wait inside a step kernel gave up (code %d); results are invalid", flag);
+    }
     return BGK_OK;
 }
 

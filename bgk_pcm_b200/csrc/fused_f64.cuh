@@ -42,6 +42,71 @@ __device__ __forceinline__ void prefetch_row(const T *F, const T *G, const TP *P
     prefetch_l2(ptr, bytes);
 }
 
+/* One node of the fused step after its pulls: momentsPre, phase_field,
+ * forces, collision, stores and (when required) moments.  Shared by the
+ * register-pull kernel below and the shared-memory pipeline kernel
+ * (fused_pipe.cuh), so both round identically. */
+template <int TANH, bool MOM, bool REF32>
+__device__ __forceinline__ void node_f64(const StepPtrs<double> &s, const Consts &c, int x, int y, long long cc,
+                                         bool E, double *f, double *g, const double (&ap)[3][3],
+                                         const double (&am)[3][3], const double *pc)
+{
+    const long long pl = s.plane;
+    /* momentsPre */
+    const double rho = sum9(f);
+    double T = sum9(g);
+    const double irho = 1.0 / rho;
+    double u = irho * xmom(f);
+    double v = irho * ymom(f);
+    const double T2 = T, u2 = u, v2 = v;
+
+    /* phase_field */
+    const double th = select_tanh(((T - c.T_crit) - c.T_act) / c.T_width, TANH);
+    const double kp = ap[1][1] + ap[1][2] + ap[2][1] + ap[1][0] + ap[0][1]
+                    + ap[2][2] + ap[2][0] + ap[0][0] + ap[0][2];
+    const double km = am[1][1] + am[1][2] + am[2][1] + am[1][0] + am[0][1]
+                    + am[2][2] + am[2][0] + am[0][0] + am[0][2];
+    const double p0 = pc[1];
+    const double phn = phi_update(c, kp, km, th, p0);
+
+    /* forces */
+    apply_forces(c, phn, p0, rho, T, u, v);
+
+    /* collision */
+    double Pq[9], eq[9], out[9];
+    eq_poly(u, v, Pq);
+#pragma unroll
+    for (int k = 0; k < 9; k++) eq[k] = c.w[k] * rho * Pq[k];
+    regularize_relax<REF32>(c, f, eq, c.omega_f, out);
+#pragma unroll
+    for (int k = 0; k < 9; k++) { s.fout[k * pl + cc] = out[k]; f[k] = out[k]; }
+#pragma unroll
+    for (int k = 0; k < 9; k++) eq[k] = c.w[k] * T * Pq[k];
+    regularize_relax<REF32>(c, g, eq, c.omega_g, out);
+#pragma unroll
+    for (int k = 0; k < 9; k++) s.gout[k * pl + cc] = out[k];
+    s.phout[cc] = phn;
+
+    /* moments (all nodes on output steps; column Nx every step) */
+    if (MOM || E) {
+        const double Tm = (sum9(out) + T2) * 0.5;
+        if (E) s.tcout[y] = Tm;
+        if (MOM) {
+            const double rm = sum9(f);
+            const double irm = 1.0 / rm;
+            const double tu = irm * xmom(f);
+            const double tv = irm * ymom(f);
+            const size_t q = (size_t)(x + 1) + (size_t)s.NX2 * (size_t)(y + 1);
+            s.mrho[q] = rm;
+            s.mT[q] = Tm;
+            s.mu[q] = (tu + u2) * 0.5;
+            s.mv[q] = (tv + v2) * 0.5;
+            s.mphi[q] = phn;
+        }
+    }
+
+}
+
 /* One thread owns one column x of a strip of H rows and marches up it.  The
  * 3x3 phi stencil is kept as per-cell selector terms (aplus/aminus) of a
  * sliding 3-row window, so each phi value is loaded and squared once per row
@@ -122,58 +187,7 @@ fused_f64_kernel(StepPtrs<double> s, Consts c, const double *__restrict__ corner
             g[7] = G[7 * pl + cp + 1];
         }
 
-        /* momentsPre */
-        const double rho = sum9(f);
-        double T = sum9(g);
-        const double irho = 1.0 / rho;
-        double u = irho * xmom(f);
-        double v = irho * ymom(f);
-        const double T2 = T, u2 = u, v2 = v;
-
-        /* phase_field */
-        const double th = select_tanh(((T - c.T_crit) - c.T_act) / c.T_width, TANH);
-        const double kp = ap[1][1] + ap[1][2] + ap[2][1] + ap[1][0] + ap[0][1]
-                        + ap[2][2] + ap[2][0] + ap[0][0] + ap[0][2];
-        const double km = am[1][1] + am[1][2] + am[2][1] + am[1][0] + am[0][1]
-                        + am[2][2] + am[2][0] + am[0][0] + am[0][2];
-        const double p0 = pc[1];
-        const double phn = phi_update(c, kp, km, th, p0);
-
-        /* forces */
-        apply_forces(c, phn, p0, rho, T, u, v);
-
-        /* collision */
-        double Pq[9], eq[9], out[9];
-        eq_poly(u, v, Pq);
-#pragma unroll
-        for (int k = 0; k < 9; k++) eq[k] = c.w[k] * rho * Pq[k];
-        regularize_relax<REF32>(c, f, eq, c.omega_f, out);
-#pragma unroll
-        for (int k = 0; k < 9; k++) { s.fout[k * pl + cc] = out[k]; f[k] = out[k]; }
-#pragma unroll
-        for (int k = 0; k < 9; k++) eq[k] = c.w[k] * T * Pq[k];
-        regularize_relax<REF32>(c, g, eq, c.omega_g, out);
-#pragma unroll
-        for (int k = 0; k < 9; k++) s.gout[k * pl + cc] = out[k];
-        s.phout[cc] = phn;
-
-        /* moments (all nodes on output steps; column Nx every step) */
-        if (MOM || E) {
-            const double Tm = (sum9(out) + T2) * 0.5;
-            if (E) s.tcout[y] = Tm;
-            if (MOM) {
-                const double rm = sum9(f);
-                const double irm = 1.0 / rm;
-                const double tu = irm * xmom(f);
-                const double tv = irm * ymom(f);
-                const size_t q = (size_t)(x + 1) + (size_t)s.NX2 * (size_t)(y + 1);
-                s.mrho[q] = rm;
-                s.mT[q] = Tm;
-                s.mu[q] = (tu + u2) * 0.5;
-                s.mv[q] = (tv + v2) * 0.5;
-                s.mphi[q] = phn;
-            }
-        }
+        node_f64<TANH, MOM, REF32>(s, c, x, y, cc, E, f, g, ap, am, pc);
 
 #pragma unroll
         for (int k = 0; k < 3; k++) {

@@ -1,0 +1,377 @@
+/*
+ * fused_pipe.cuh -- the fused step with a shared-memory pipeline.
+ *
+ * The register-pull kernel (fused_f64.cuh) issues its 18 population loads and
+ * then computes: with ~128 registers per thread only ~16 warps fit on an SM,
+ * and the loads of a warp are not in flight while it computes, so the kernel
+ * is latency-bound below the HBM roofline.  Here the loads are decoupled:
+ *
+ *  - one producer warp per CTA streams, for each row the CTA will compute,
+ *    the 18 population row-segments (f and g planes, each at its pull source
+ *    row y - c_y, clamped into the domain) and the next phi row into a ring of
+ *    D shared-memory stages with bulk asynchronous copies (cp.async.bulk,
+ *    completion counted in bytes on a per-stage mbarrier);
+ *  - four consumer warps (one node per thread) wait for a stage, pull their
+ *    populations from shared memory (x +/- 1 is a neighbouring word, no
+ *    misaligned global access), compute the node with the same device
+ *    function as the register-pull kernel (node_f64), write the results and
+ *    release the stage on a second mbarrier.
+ * A CTA owns tiles of 128 columns x H rows (persistent, round-robin); the
+ * producer runs D rows ahead across tile boundaries.  Row segments start 16
+ * bytes before the band (the population buffers carry 256-byte guards), so
+ * every copy is 16-byte aligned.  Boundary nodes read their bounce-back and
+ * boundary values from global memory, as in the register-pull kernel.
+ *
+ * Every wait is bounded (about a second); on expiry the thread records a code
+ * in errflag and leaves its loop, and the producer waits (bounded) for all of
+ * its copies before it exits.  No multicast, no clusters.
+ *
+ * Include inside an anonymous namespace in namespace bgk after fused_f64.cuh.
+ */
+#ifndef BGK_FUSED_PIPE_CUH
+#define BGK_FUSED_PIPE_CUH
+
+constexpr int PIPE_BX = 128;
+constexpr int PIPE_CWARPS = PIPE_BX / 32;
+constexpr int PIPE_THREADS = PIPE_BX + 32;
+constexpr long long PIPE_WAIT_LIMIT = 1LL << 24;   /* x ~64 ns sleeps: ~1 s */
+
+struct PipeSched {
+    int nbands, H, nstrips, ntiles;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+
+/* Bounded wait: false after ~PIPE_WAIT_LIMIT polls. */
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+{
+    for (long long i = 0; i < PIPE_WAIT_LIMIT; i++) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (i > 32) __nanosleep(64);
+    }
+    return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+/* Stage geometry for storage type S (populations) and PT (phi). */
+template <typename S, typename PT>
+struct PipeGeom {
+    static constexpr int AL = 16 / (int)sizeof(S);       /* left pad (elements) */
+    static constexpr int RW = PIPE_BX + 2 * AL;
+    static constexpr int ALP = 16 / (int)sizeof(PT);
+    static constexpr int RWP = PIPE_BX + 2 * ALP;
+    static constexpr int POP_BYTES = RW * (int)sizeof(S);
+    static constexpr int PHI_BYTES = RWP * (int)sizeof(PT);
+    static constexpr int STAGE_BYTES = (18 * POP_BYTES + PHI_BYTES + 127) / 128 * 128;
+    static constexpr int TX_BYTES = 18 * POP_BYTES + PHI_BYTES;
+    static constexpr int HEADER = 256;                    /* mbarriers (2 x 16 max) */
+    static size_t smem_bytes(int D) { return (size_t)HEADER + (size_t)D * STAGE_BYTES; }
+};
+
+__constant__ int pipe_cy[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
+
+/* Producer: issue the 19 row-segment copies of work item (x0, y) into a stage. */
+template <typename S, typename PT>
+__device__ __forceinline__ void pipe_issue(const S *F, const S *G, const PT *PH, long long pl, int P, int Ny, int x0,
+                                           int y, unsigned char *stage, uint64_t *full)
+{
+    using Gm = PipeGeom<S, PT>;
+    mbar_arrive_expect_tx(full, Gm::TX_BYTES);
+#pragma unroll 1
+    for (int k = 0; k < 9; k++) {
+        int r = y - pipe_cy[k];
+        r = r < 0 ? 0 : (r >= Ny ? Ny - 1 : r);
+        const long long off = (long long)r * P + x0 - Gm::AL;
+        bulk_g2s(stage + k * Gm::POP_BYTES, F + k * pl + off, Gm::POP_BYTES, full);
+        bulk_g2s(stage + (9 + k) * Gm::POP_BYTES, G + k * pl + off, Gm::POP_BYTES, full);
+    }
+    const int rp = (y + 1 >= Ny) ? Ny - 1 : y + 1;
+    bulk_g2s(stage + 18 * Gm::POP_BYTES, PH + (long long)rp * P + x0 - Gm::ALP, Gm::PHI_BYTES, full);
+}
+
+/* Iterate this CTA's work items in order: tiles t = blockIdx.x, +gridDim.x,
+ * ..., rows y0..y1-1 of each.  next() returns false at the end. */
+struct PipeIter {
+    int t, y, y1, x0;
+    PipeSched sch;
+    int Ny;
+    __device__ bool start(const PipeSched &s, int Ny_)
+    {
+        sch = s;
+        Ny = Ny_;
+        t = blockIdx.x;
+        return open();
+    }
+    __device__ bool open()
+    {
+        if (t >= sch.ntiles) return false;
+        const int band = t % sch.nbands, strip = t / sch.nbands;
+        x0 = band * PIPE_BX;
+        y = strip * sch.H;
+        y1 = min(y + sch.H, Ny);
+        return true;
+    }
+    __device__ bool next()
+    {
+        if (++y < y1) return true;
+        t += gridDim.x;
+        return open();
+    }
+};
+
+template <int D, int TANH, bool MOM, bool REF32>
+__global__ void __launch_bounds__(PIPE_THREADS, 3)
+fused_pipe_f64_kernel(StepPtrs<double> s, Consts c, const double *__restrict__ corner, PipeSched sch, int *errflag)
+{
+    using Gm = PipeGeom<double, double>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem);
+    uint64_t *empty = full + D;
+    unsigned char *stages = smem + Gm::HEADER;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int Nx = c.Nx, Ny = c.Ny;
+    if (tid == 0) {
+        for (int d = 0; d < D; d++) {
+            mbar_init(&full[d], 1);
+            mbar_init(&empty[d], PIPE_CWARPS);
+        }
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    if (warp == PIPE_CWARPS) {
+        /* ---------------- producer ---------------- */
+        if (lane != 0) return;
+        PipeIter it;
+        long long r = 0;
+        bool ok = it.start(sch, Ny);
+        while (ok) {
+            const int st = (int)(r % D);
+            if (r >= D && !mbar_wait(&empty[st], (uint32_t)(((r / D) - 1) & 1))) {
+                atomicExch(errflag, 1);
+                break;
+            }
+            pipe_issue<double, double>(s.fin, s.gin, s.phin, s.plane, s.P, Ny, it.x0, it.y,
+                                       stages + (size_t)st * Gm::STAGE_BYTES, &full[st]);
+            r++;
+            ok = it.next();
+        }
+        /* do not retire while copies into this CTA's shared memory are in flight */
+        for (long long q = (r > D ? r - D : 0); q < r; q++)
+            if (!mbar_wait(&full[q % D], (uint32_t)((q / D) & 1))) atomicExch(errflag, 2);
+        return;
+    }
+
+    /* ---------------- consumers ---------------- */
+    const long long pl = s.plane;
+    const int P = s.P;
+    const double *__restrict__ F = s.fin;
+    const double *__restrict__ PH = s.phin;
+    PipeIter it;
+    long long r = 0;
+    bool ok = it.start(sch, Ny);
+    while (ok) {
+        const int x = it.x0 + tid;
+        const bool active = x < Nx;
+        const bool W = (x == 0), E = (x == Nx - 1);
+        double ap[3][3], am[3][3], pc[3];
+        if (active) {
+            for (int slot = 0; slot < 2; slot++) {
+                const int rr = it.y - 1 + slot;
+                const int rc = rr < 0 ? 0 : (rr >= Ny ? Ny - 1 : rr);
+                const double *row = PH + (long long)rc * P;
+                const double pL = W ? s.phiW[rc] : row[x - 1];
+                const double pM = row[x];
+                const double pR = E ? s.phiE[rc] : row[x + 1];
+                ap[slot][0] = aplus(pL); ap[slot][1] = aplus(pM); ap[slot][2] = aplus(pR);
+                am[slot][0] = aminus(pL); am[slot][1] = aminus(pM); am[slot][2] = aminus(pR);
+                pc[slot] = pM;
+            }
+        }
+        const int tile = it.t;
+        bool failed = false;
+        do {
+            const int y = it.y;
+            const int st = (int)(r % D);
+            if (!mbar_wait(&full[st], (uint32_t)((r / D) & 1))) {
+                atomicExch(errflag, 3);
+                failed = true;
+                break;
+            }
+            const double *stg = reinterpret_cast<const double *>(stages + (size_t)st * Gm::STAGE_BYTES);
+            const double *sp = stg;                                    /* f planes */
+            const double *sg = stg + 9 * Gm::RW;                       /* g planes */
+            const double *sphi = stg + 18 * Gm::RW;
+            if (active) {
+                const bool S = (y == 0), N = (y == Ny - 1);
+                const long long cc = (long long)y * P + x;
+                const int col = tid + Gm::AL;
+                /* new phi row y+1 of the window */
+                {
+                    const int rc = (y + 1 >= Ny) ? Ny - 1 : y + 1;
+                    const double pL = W ? s.phiW[rc] : sphi[Gm::ALP + tid - 1];
+                    const double pM = sphi[Gm::ALP + tid];
+                    const double pR = E ? s.phiE[rc] : sphi[Gm::ALP + tid + 1];
+                    ap[2][0] = aplus(pL); ap[2][1] = aplus(pM); ap[2][2] = aplus(pR);
+                    am[2][0] = aminus(pL); am[2][1] = aminus(pM); am[2][2] = aminus(pR);
+                    pc[2] = pM;
+                }
+                double f[9], g[9];
+                f[0] = sp[0 * Gm::RW + col];
+                f[1] = W ? sp[3 * Gm::RW + col] : sp[1 * Gm::RW + col - 1];
+                f[2] = sp[2 * Gm::RW + col];
+                f[3] = E ? sp[1 * Gm::RW + col] : sp[3 * Gm::RW + col + 1];
+                f[4] = sp[4 * Gm::RW + col];
+                f[5] = sp[5 * Gm::RW + col - 1];
+                f[6] = sp[6 * Gm::RW + col + 1];
+                f[7] = sp[7 * Gm::RW + col + 1];
+                f[8] = sp[8 * Gm::RW + col - 1];
+                if (W || E || S || N) {
+                    /* bounce-back values that are not in the stage */
+                    if (S) f[2] = F[4 * pl + cc];
+                    if (N) f[4] = F[2 * pl + cc];
+                    if (W || S) f[5] = F[7 * pl + cc];
+                    if (E || S) f[6] = (E && S) ? corner[0] : F[8 * pl + cc];
+                    if (E || N) f[7] = (E && N) ? corner[1] : F[5 * pl + cc];
+                    if (W || N) f[8] = F[6 * pl + cc];
+                }
+                const int ym = S ? y : y - 1, yp = N ? y : y + 1;
+                g[0] = sg[0 * Gm::RW + col];
+                g[2] = sg[2 * Gm::RW + col];
+                g[4] = sg[4 * Gm::RW + col];
+                if (W) {
+                    g[1] = s.gW[y];
+                    g[5] = s.gW[Ny + ym];
+                    g[8] = s.gW[2 * Ny + yp];
+                } else {
+                    g[1] = sg[1 * Gm::RW + col - 1];
+                    g[5] = sg[5 * Gm::RW + col - 1];
+                    g[8] = sg[8 * Gm::RW + col - 1];
+                }
+                if (E) {
+                    g[3] = c.w[3] * s.tcin[y] * s.pE[y];
+                    g[6] = c.w[6] * s.tcin[ym] * s.pE[Ny + ym];
+                    g[7] = c.w[7] * s.tcin[yp] * s.pE[2 * Ny + yp];
+                } else {
+                    g[3] = sg[3 * Gm::RW + col + 1];
+                    g[6] = sg[6 * Gm::RW + col + 1];
+                    g[7] = sg[7 * Gm::RW + col + 1];
+                }
+                node_f64<TANH, MOM, REF32>(s, c, x, y, cc, E, f, g, ap, am, pc);
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    ap[0][k] = ap[1][k]; ap[1][k] = ap[2][k];
+                    am[0][k] = am[1][k]; am[1][k] = am[2][k];
+                }
+                pc[0] = pc[1]; pc[1] = pc[2];
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[st]);
+            r++;
+            ok = it.next();
+        } while (ok && it.t == tile);
+        if (failed) break;
+    }
+}
+
+inline PipeSched pipe_sched(const bgk_ctx *c, int ctas_per_sm, int *grid)
+{
+    PipeSched sch;
+    sch.nbands = (c->Nx + PIPE_BX - 1) / PIPE_BX;
+    const long long slots = (long long)c->nsm * ctas_per_sm;
+    /* strips short enough for at least ~6 tiles per resident CTA */
+    int H = 64;
+    while (H > 8 && (long long)sch.nbands * ((c->Ny + H - 1) / H) < 6 * slots) H /= 2;
+    if (c->tune_H > 0) H = c->tune_H;
+    sch.H = H;
+    sch.nstrips = (c->Ny + H - 1) / H;
+    sch.ntiles = sch.nbands * sch.nstrips;
+    *grid = (int)(sch.ntiles < slots ? sch.ntiles : slots);
+    return sch;
+}
+
+template <int D, int T, bool M, bool R>
+inline cudaError_t pipe_f64_launch(const bgk_ctx *c, const StepPtrs<double> &s, int ctas)
+{
+    using Gm = PipeGeom<double, double>;
+    const size_t smem = Gm::smem_bytes(D);
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(fused_pipe_f64_kernel<D, T, M, R>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    int grid;
+    const PipeSched sch = pipe_sched(c, ctas, &grid);
+    fused_pipe_f64_kernel<D, T, M, R><<<grid, PIPE_THREADS, smem, c->stream>>>(s, c->c, c->corner, sch, c->errflag);
+    return cudaGetLastError();
+}
+
+template <int D>
+inline cudaError_t pipe_f64_dispatch(const bgk_ctx *c, const StepPtrs<double> &s, bool mom, int ctas)
+{
+    const bool portable = c->opt.tanh_mode == BGK_TANH_PORTABLE;
+    const bool ref32 = !c->opt.smooth;
+    if (portable) {
+        if (mom) return ref32 ? pipe_f64_launch<D, BGK_TANH_PORTABLE, true, true>(c, s, ctas)
+                              : pipe_f64_launch<D, BGK_TANH_PORTABLE, true, false>(c, s, ctas);
+        return ref32 ? pipe_f64_launch<D, BGK_TANH_PORTABLE, false, true>(c, s, ctas)
+                     : pipe_f64_launch<D, BGK_TANH_PORTABLE, false, false>(c, s, ctas);
+    }
+    if (mom) return ref32 ? pipe_f64_launch<D, BGK_TANH_DEVICE, true, true>(c, s, ctas)
+                          : pipe_f64_launch<D, BGK_TANH_DEVICE, true, false>(c, s, ctas);
+    return ref32 ? pipe_f64_launch<D, BGK_TANH_DEVICE, false, true>(c, s, ctas)
+                 : pipe_f64_launch<D, BGK_TANH_DEVICE, false, false>(c, s, ctas);
+}
+
+/* Pipeline depth 2..4 stages of ~20 KB; CTAs per SM from the shared memory
+ * budget unless overridden. */
+inline cudaError_t launch_fused_pipe_f64(const bgk_ctx *c, const StepPtrs<double> &s, bool mom)
+{
+    const int D = c->tune_D > 0 ? c->tune_D : 3;
+    const int ctas = c->tune_ctas > 0 ? c->tune_ctas : (D <= 2 ? 4 : (D == 3 ? 3 : 2));
+    switch (D) {
+    case 2: return pipe_f64_dispatch<2>(c, s, mom, ctas);
+    case 4: return pipe_f64_dispatch<4>(c, s, mom, ctas);
+    default: return pipe_f64_dispatch<3>(c, s, mom, ctas);
+    }
+}
+
+#endif

@@ -148,6 +148,7 @@ __global__ void macro_halo_kernel(Consts c, double *rho, double *T, double *u, d
 }
 
 #include "fused_f64.cuh"
+#include "fused_pipe.cuh"
 
 /* --------------------------------------------------------- staged kernels */
 
@@ -616,6 +617,7 @@ cudaError_t launch_fused_f64(bgk_ctx *c, bool moments)
     dim3 grd((c->Nx + FUSED_BX - 1) / FUSED_BX, (c->Ny + H - 1) / H);
     const double *corner = corner_ptr(c);
     (void)corner;
+    if (c->tune_pipe) return launch_fused_pipe_f64(c, s, moments);
     return launch_fused_f64_variant(c, grd, s, H, moments);
 }
 
@@ -632,6 +634,7 @@ cudaError_t launch_fused_f64_ptrs(bgk_ctx *c, const double *fin, const double *g
     s.plane = c->plane; s.P = c->P; s.NX2 = c->NX2;
     const int H = strip_height(c);
     dim3 grd((c->Nx + FUSED_BX - 1) / FUSED_BX, (c->Ny + H - 1) / H);
+    if (c->tune_pipe) return launch_fused_pipe_f64(c, s, false);
     return launch_fused_f64_variant(c, grd, s, H, false);
 }
 

@@ -20,6 +20,7 @@ __device__ __forceinline__ double select_tanh(double x, int mode)
 }
 
 #include "fused_f64.cuh"
+#include "fused_pipe.cuh"
 
 int strip_height(const bgk_ctx *c)
 {
@@ -48,6 +49,7 @@ cudaError_t launch_fused_fast(bgk_ctx *c, bool moments)
     s.plane = c->plane; s.P = c->P; s.NX2 = c->NX2;
     const int H = strip_height(c);
     dim3 grd((c->Nx + FUSED_BX - 1) / FUSED_BX, (c->Ny + H - 1) / H);
+    if (c->tune_pipe) return launch_fused_pipe_f64(c, s, moments);
     return launch_fused_f64_variant(c, grd, s, H, moments);
 }
 
