@@ -419,9 +419,13 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
     cudaStream_t st = c->stream;
     const long long pl = c->plane;
     const int Ny = c->Ny;
-    /* one stored state: f (9 planes), g (9), phi (1), T column (Ny, padded) */
+    /* one stored state: f (9 planes), g (9), phi (1), T column (Ny, padded),
+     * with a guard before and after it: the fused step's shared-memory
+     * pipeline copies row segments that start 16 bytes before a band and may
+     * run up to a band (128 elements) past the last row of a plane */
     const long long tc_pad = ((long long)Ny + 31) / 32 * 32;
-    const size_t state_elems = (size_t)(19 * pl + tc_pad);
+    const size_t state_guard = 256;     /* elements on each side */
+    const size_t state_elems = (size_t)(19 * pl + tc_pad) + 2 * state_guard;
     const int nsnap = (N + K - 1) / K;    /* snapshots of S(0), S(K), ...    */
     std::vector<void *> allocs;
     auto dmalloc = [&](size_t bytes) -> double * {
@@ -431,8 +435,10 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
         return (double *)p;
     };
     auto cleanup = [&]() { for (void *p : allocs) cudaFree(p); };
-    double *snaps = dmalloc((size_t)nsnap * state_elems * sizeof(double));
-    double *seg = dmalloc((size_t)(K + 1) * state_elems * sizeof(double));
+    double *snaps_raw = dmalloc((size_t)nsnap * state_elems * sizeof(double));
+    double *seg_raw = dmalloc((size_t)(K + 1) * state_elems * sizeof(double));
+    double *snaps = snaps_raw ? snaps_raw + state_guard : nullptr;   /* state i at snaps + i*state_elems */
+    double *seg = seg_raw ? seg_raw + state_guard : nullptr;
     double *pi[2] = {dmalloc((size_t)NPI * pl * sizeof(double)), dmalloc((size_t)NPI * pl * sizeof(double))};
     dim3 blk(AB_X, AB_Y), grd((c->Nx + AB_X - 1) / AB_X, (Ny + AB_Y - 1) / AB_Y);
     const int nblk = grd.x * grd.y;
@@ -493,7 +499,7 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
         const int n0 = sgi * K;
         const int n1 = (n0 + K < N) ? n0 + K : N;
         /* states S(n0) .. S(n1-1) into seg[0 .. n1-n0-1] */
-        ACK(cudaMemcpyAsync(seg, snaps + (size_t)sgi * state_elems, state_elems * sizeof(double),
+        ACK(cudaMemcpyAsync(seg, snaps + (size_t)sgi * state_elems, (state_elems - 2 * state_guard) * sizeof(double),
                             cudaMemcpyDeviceToDevice, st));
         for (int n = n0 + 1; n < n1; n++) {
             double *a = seg + (size_t)(n - 1 - n0) * state_elems;

@@ -361,12 +361,14 @@ inline cudaError_t pipe_f64_dispatch(const bgk_ctx *c, const StepPtrs<double> &s
                  : pipe_f64_launch<D, BGK_TANH_DEVICE, false, false>(c, s, ctas);
 }
 
-/* Pipeline depth 2..4 stages of ~20 KB; CTAs per SM from the shared memory
- * budget unless overridden. */
+/* Pipeline depth 2..4 stages of ~20 KB.  Measured on B200 at 2048^2 and
+ * 4096^2: 2 stages with 3 CTAs per SM (12 consumer warps) is best (92 % /
+ * 88 % of the copy bandwidth); more stages or CTAs lose occupancy or issue
+ * slots. */
 inline cudaError_t launch_fused_pipe_f64(const bgk_ctx *c, const StepPtrs<double> &s, bool mom)
 {
-    const int D = c->tune_D > 0 ? c->tune_D : 3;
-    const int ctas = c->tune_ctas > 0 ? c->tune_ctas : (D <= 2 ? 4 : (D == 3 ? 3 : 2));
+    const int D = c->tune_D > 0 ? c->tune_D : 2;
+    const int ctas = c->tune_ctas > 0 ? c->tune_ctas : (D <= 2 ? 3 : 2);
     switch (D) {
     case 2: return pipe_f64_dispatch<2>(c, s, mom, ctas);
     case 4: return pipe_f64_dispatch<4>(c, s, mom, ctas);

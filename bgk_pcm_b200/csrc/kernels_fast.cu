@@ -68,17 +68,18 @@ namespace {
  * which is the reference's ft - omega (ft - feq) without forming ft.
  * ---------------------------------------------------------------------- */
 
+template <typename AT>
 struct ConstsLP {
     int Nx, Ny;
-    float w[9];
-    float cf[9], cg[9];      /* (1 - omega) * (0.5 w_k / cs2^2)             */
-    float m, q;              /* -cs2, 1 - cs2                                */
-    float rho0, T0;
-    float T0mTcrit;          /* T0 - T_crit                                  */
-    float inv_T_width;
-    float f_plus, f_minus;
-    float gb;                /* grav * beta                                  */
-    float omega_f;
+    AT w[9];
+    AT cf[9], cg[9];         /* (1 - omega) * (0.5 w_k / cs2^2)             */
+    AT m, q;                 /* -cs2, 1 - cs2                                */
+    AT rho0, T0;
+    AT T0mTcrit;             /* T0 - T_crit                                  */
+    AT inv_T_width;
+    AT f_plus, f_minus;
+    AT gb;                   /* grav * beta                                  */
+    AT omega_f;
     double dts, T0d, rho0d;
     double T0mTcrit_d, inv_T_width_d;
     double w_d[9];
@@ -103,36 +104,39 @@ __device__ __forceinline__ float tanh_lp(float x, int mode)
     return mode == BGK_TANH_PORTABLE ? (float)bgk_portable_tanh((double)x) : tanhf(x);
 }
 
-__device__ __forceinline__ void qpoly(float u, float v, float *Q)
+template <typename AT>
+__device__ __forceinline__ void qpoly(AT u, AT v, AT *Q)
 {
-    const float uu = u * u, vv = v * v, uv = 1.5f * (uu + vv);
-    const float upv = u + v, umv = u - v;
+    const AT uu = u * u, vv = v * v, uv = (AT)1.5 * (uu + vv);
+    const AT upv = u + v, umv = u - v;
+    const AT three = (AT)3, f45 = (AT)4.5;
     Q[0] = -uv;
-    Q[1] = 3.0f * u + 4.5f * uu - uv;
-    Q[2] = 3.0f * v + 4.5f * vv - uv;
-    Q[3] = -3.0f * u + 4.5f * uu - uv;
-    Q[4] = -3.0f * v + 4.5f * vv - uv;
-    Q[5] = 3.0f * upv + 4.5f * upv * upv - uv;
-    Q[6] = -3.0f * umv + 4.5f * umv * umv - uv;
-    Q[7] = -3.0f * upv + 4.5f * upv * upv - uv;
-    Q[8] = 3.0f * umv + 4.5f * umv * umv - uv;
+    Q[1] = three * u + f45 * uu - uv;
+    Q[2] = three * v + f45 * vv - uv;
+    Q[3] = -three * u + f45 * uu - uv;
+    Q[4] = -three * v + f45 * vv - uv;
+    Q[5] = three * upv + f45 * upv * upv - uv;
+    Q[6] = -three * umv + f45 * umv * umv - uv;
+    Q[7] = -three * upv + f45 * upv * upv - uv;
+    Q[8] = three * umv + f45 * umv * umv - uv;
 }
 
-__device__ __forceinline__ void reg_relax_lp(const ConstsLP &c, const float *in, const float *eq,
-                                             const float *cc, float *out)
+template <typename AT>
+__device__ __forceinline__ void reg_relax_lp(const ConstsLP<AT> &c, const AT *in, const AT *eq, const AT *cc,
+                                             AT *out)
 {
-    float d[9];
+    AT d[9];
 #pragma unroll
     for (int k = 0; k < 9; k++) d[k] = in[k] - eq[k];
-    const float m = c.m, q = c.q;
-    const float pxx = m * (d[0] + d[2] + d[4]) + q * (d[1] + d[3] + d[5] + d[6] + d[7] + d[8]);
-    const float pyy = m * (d[0] + d[1] + d[3]) + q * (d[2] + d[4] + d[5] + d[6] + d[7] + d[8]);
-    const float pxy = d[5] - d[6] + d[7] - d[8];
-    const float s0 = m * (pxx + pyy);
-    const float s1 = q * pxx + m * pyy;
-    const float s2 = m * pxx + q * pyy;
-    const float sqq = q * (pxx + pyy);
-    const float s5 = sqq + 2.0f * pxy, s6 = sqq - 2.0f * pxy;
+    const AT m = c.m, q = c.q;
+    const AT pxx = m * (d[0] + d[2] + d[4]) + q * (d[1] + d[3] + d[5] + d[6] + d[7] + d[8]);
+    const AT pyy = m * (d[0] + d[1] + d[3]) + q * (d[2] + d[4] + d[5] + d[6] + d[7] + d[8]);
+    const AT pxy = d[5] - d[6] + d[7] - d[8];
+    const AT s0 = m * (pxx + pyy);
+    const AT s1 = q * pxx + m * pyy;
+    const AT s2 = m * pxx + q * pyy;
+    const AT sqq = q * (pxx + pyy);
+    const AT s5 = sqq + (AT)2 * pxy, s6 = sqq - (AT)2 * pxy;
     out[0] = eq[0] + cc[0] * s0;
     out[1] = eq[1] + cc[1] * s1;
     out[2] = eq[2] + cc[2] * s2;
@@ -172,9 +176,89 @@ __device__ __forceinline__ double tanh_pt<double>(double x, int mode)
     return mode == BGK_TANH_PORTABLE ? bgk_portable_tanh(x) : tanh(x);
 }
 
-template <typename S, typename PT, int TANH, bool MOM>
+/* One node of a reduced-precision step after its pulls (deviations in AT):
+ * momentsPre, phase field (PT), latent heat (FP64), forces, collision,
+ * stores, moments.  Shared by the register-pull and pipeline kernels. */
+template <typename S, typename PT, typename AT, int TANH, bool MOM>
+__device__ __forceinline__ void node_lp(const LpPtrs<S, PT> &s, const ConstsLP<AT> &c, int x, int y, long long cc,
+                                        bool E, AT *f, AT *g, const PT (&ap)[3][3], const PT (&am)[3][3],
+                                        const PT *pc)
+{
+    using C = Codec<S>;
+    const long long pl = s.plane;
+    /* momentsPre (deviations) */
+    AT drho = 0, dT = 0;
+#pragma unroll
+    for (int k = 0; k < 9; k++) { drho += f[k]; dT += g[k]; }
+    const AT rho = c.rho0 + drho;
+    const AT irho = (AT)1 / rho;
+    AT u = irho * (f[1] - f[3] + f[5] - f[6] - f[7] + f[8]);
+    AT v = irho * (f[2] - f[4] + f[5] + f[6] - f[7] - f[8]);
+    const AT dT2 = dT, u2 = u, v2 = v;
+
+    /* phase_field (in PT) */
+    const PT one = (PT)1, half = (PT)0.5;
+    const PT th = tanh_pt<PT>(((PT)c.T0mTcrit_d + (PT)dT) * (PT)c.inv_T_width_d, TANH);
+    const PT kp = ap[1][1] + ap[1][2] + ap[2][1] + ap[1][0] + ap[0][1] + ap[2][2] + ap[2][0] + ap[0][0] + ap[0][2];
+    const PT km = am[1][1] + am[1][2] + am[2][1] + am[1][0] + am[0][1] + am[2][2] + am[2][0] + am[0][0] + am[0][2];
+    const PT p0 = pc[1];
+    const PT kpp = kp * (PT)0.125 * (half * (one + th));
+    const PT kmm = km * (PT)0.125 * (half * (one - th));
+    const PT phn_p = p0 + (half * kpp * (one - p0) - half * kmm * (one + p0));
+    const AT phn = (AT)phn_p;
+
+    /* forces: latent heat in FP64 */
+    dT = (AT)((double)dT - c.dts * ((double)phn_p - (double)p0) * 0.5);
+    const AT T = c.T0 + dT;
+    const AT omp = (AT)1 - phn;
+    const AT forceY = rho * c.gb * T * ((AT)1 + (AT)0.5 * phn) - (AT)0.5 * v * omp;
+    const AT forceX = (AT)-0.5 * u * omp;
+    const AT iw = (AT)1 / (c.omega_f * rho);
+    u = u + forceX * iw;
+    v = v + forceY * iw;
+
+    /* collision */
+    AT Q[9], eq[9], out[9];
+    qpoly(u, v, Q);
+#pragma unroll
+    for (int k = 0; k < 9; k++) eq[k] = c.w[k] * (c.rho0 * Q[k] + drho * ((AT)1 + Q[k]));
+    reg_relax_lp(c, f, eq, c.cf, out);
+#pragma unroll
+    for (int k = 0; k < 9; k++) { C::st(s.fout + k * pl + cc, (float)out[k], s.sf); f[k] = out[k]; }
+#pragma unroll
+    for (int k = 0; k < 9; k++) eq[k] = c.w[k] * (c.T0 * Q[k] + dT * ((AT)1 + Q[k]));
+    reg_relax_lp(c, g, eq, c.cg, out);
+#pragma unroll
+    for (int k = 0; k < 9; k++) C::st(s.gout + k * pl + cc, (float)out[k], s.sg);
+    s.phout[cc] = phn_p;
+
+    if (MOM || E) {
+        AT sg = 0;
+#pragma unroll
+        for (int k = 0; k < 9; k++) sg += out[k];
+        const double Tm = c.T0d + 0.5 * ((double)sg + (double)dT2);
+        if (E) s.tcout[y] = Tm;
+        if (MOM) {
+            AT sf = 0;
+#pragma unroll
+            for (int k = 0; k < 9; k++) sf += f[k];
+            const AT rm = c.rho0 + sf;
+            const AT irm = (AT)1 / rm;
+            const AT tu = irm * (f[1] - f[3] + f[5] - f[6] - f[7] + f[8]);
+            const AT tv = irm * (f[2] - f[4] + f[5] + f[6] - f[7] - f[8]);
+            const size_t q = (size_t)(x + 1) + (size_t)s.NX2 * (size_t)(y + 1);
+            s.mrho[q] = (double)c.rho0 + (double)sf;
+            s.mT[q] = Tm;
+            s.mu[q] = 0.5 * ((double)tu + (double)u2);
+            s.mv[q] = 0.5 * ((double)tv + (double)v2);
+            s.mphi[q] = (double)phn_p;
+        }
+    }
+}
+
+template <typename S, typename PT, typename AT, int TANH, bool MOM>
 __global__ void __launch_bounds__(FUSED_BX)
-fused_lowp_kernel(LpPtrs<S, PT> s, ConstsLP c, int H, int pf)
+fused_lowp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, int H, int pf)
 {
     const int Nx = c.Nx, Ny = c.Ny;
     const int x = blockIdx.x * FUSED_BX + threadIdx.x;
@@ -212,112 +296,46 @@ fused_lowp_kernel(LpPtrs<S, PT> s, ConstsLP c, int H, int pf)
         load_row(y + 1, 2);
         const bool Sb = (y == 0), N = (y == Ny - 1);
         const long long cc = (long long)y * P + x;
-        float f[9], g[9];
+        AT f[9], g[9];
         using C = Codec<S>;
-        f[0] = C::ld(F + cc, isf);
-        f[1] = C::ld(W ? F + 3 * pl + cc : F + 1 * pl + cc - 1, isf);
-        f[2] = C::ld(Sb ? F + 4 * pl + cc : F + 2 * pl + cc - P, isf);
-        f[3] = C::ld(E ? F + 1 * pl + cc : F + 3 * pl + cc + 1, isf);
-        f[4] = C::ld(N ? F + 2 * pl + cc : F + 4 * pl + cc + P, isf);
-        f[5] = C::ld((W || Sb) ? F + 7 * pl + cc : F + 5 * pl + cc - P - 1, isf);
-        f[6] = C::ld((E || Sb) ? F + 8 * pl + cc : F + 6 * pl + cc - P + 1, isf);
-        f[7] = C::ld((E || N) ? F + 5 * pl + cc : F + 7 * pl + cc + P + 1, isf);
-        f[8] = C::ld((W || N) ? F + 6 * pl + cc : F + 8 * pl + cc + P - 1, isf);
-        if (E && Sb) f[6] = (float)(s.corner[0] - c.w_d[6] * c.rho0d);
-        if (E && N) f[7] = (float)(s.corner[1] - c.w_d[7] * c.rho0d);
+        f[0] = (AT)C::ld(F + cc, isf);
+        f[1] = (AT)C::ld(W ? F + 3 * pl + cc : F + 1 * pl + cc - 1, isf);
+        f[2] = (AT)C::ld(Sb ? F + 4 * pl + cc : F + 2 * pl + cc - P, isf);
+        f[3] = (AT)C::ld(E ? F + 1 * pl + cc : F + 3 * pl + cc + 1, isf);
+        f[4] = (AT)C::ld(N ? F + 2 * pl + cc : F + 4 * pl + cc + P, isf);
+        f[5] = (AT)C::ld((W || Sb) ? F + 7 * pl + cc : F + 5 * pl + cc - P - 1, isf);
+        f[6] = (AT)C::ld((E || Sb) ? F + 8 * pl + cc : F + 6 * pl + cc - P + 1, isf);
+        f[7] = (AT)C::ld((E || N) ? F + 5 * pl + cc : F + 7 * pl + cc + P + 1, isf);
+        f[8] = (AT)C::ld((W || N) ? F + 6 * pl + cc : F + 8 * pl + cc + P - 1, isf);
+        if (E && Sb) f[6] = (AT)(s.corner[0] - c.w_d[6] * c.rho0d);
+        if (E && N) f[7] = (AT)(s.corner[1] - c.w_d[7] * c.rho0d);
 
         const int ym = Sb ? y : y - 1, yp = N ? y : y + 1;
         const long long cm = (long long)ym * P + x, cp = (long long)yp * P + x;
-        g[0] = C::ld(G + cc, isg);
-        g[2] = C::ld(G + 2 * pl + cm, isg);
-        g[4] = C::ld(G + 4 * pl + cp, isg);
+        g[0] = (AT)C::ld(G + cc, isg);
+        g[2] = (AT)C::ld(G + 2 * pl + cm, isg);
+        g[4] = (AT)C::ld(G + 4 * pl + cp, isg);
         if (W) {
-            g[1] = (float)(s.gW[y] - c.w_d[1] * c.T0d);
-            g[5] = (float)(s.gW[Ny + ym] - c.w_d[5] * c.T0d);
-            g[8] = (float)(s.gW[2 * Ny + yp] - c.w_d[8] * c.T0d);
+            g[1] = (AT)(s.gW[y] - c.w_d[1] * c.T0d);
+            g[5] = (AT)(s.gW[Ny + ym] - c.w_d[5] * c.T0d);
+            g[8] = (AT)(s.gW[2 * Ny + yp] - c.w_d[8] * c.T0d);
         } else {
-            g[1] = C::ld(G + 1 * pl + cc - 1, isg);
-            g[5] = C::ld(G + 5 * pl + cm - 1, isg);
-            g[8] = C::ld(G + 8 * pl + cp - 1, isg);
+            g[1] = (AT)C::ld(G + 1 * pl + cc - 1, isg);
+            g[5] = (AT)C::ld(G + 5 * pl + cm - 1, isg);
+            g[8] = (AT)C::ld(G + 8 * pl + cp - 1, isg);
         }
         if (E) {
-            g[3] = (float)(c.w_d[3] * s.tcin[y] * s.pE[y] - c.w_d[3] * c.T0d);
-            g[6] = (float)(c.w_d[6] * s.tcin[ym] * s.pE[Ny + ym] - c.w_d[6] * c.T0d);
-            g[7] = (float)(c.w_d[7] * s.tcin[yp] * s.pE[2 * Ny + yp] - c.w_d[7] * c.T0d);
+            g[3] = (AT)(c.w_d[3] * s.tcin[y] * s.pE[y] - c.w_d[3] * c.T0d);
+            g[6] = (AT)(c.w_d[6] * s.tcin[ym] * s.pE[Ny + ym] - c.w_d[6] * c.T0d);
+            g[7] = (AT)(c.w_d[7] * s.tcin[yp] * s.pE[2 * Ny + yp] - c.w_d[7] * c.T0d);
         } else {
-            g[3] = C::ld(G + 3 * pl + cc + 1, isg);
-            g[6] = C::ld(G + 6 * pl + cm + 1, isg);
-            g[7] = C::ld(G + 7 * pl + cp + 1, isg);
+            g[3] = (AT)C::ld(G + 3 * pl + cc + 1, isg);
+            g[6] = (AT)C::ld(G + 6 * pl + cm + 1, isg);
+            g[7] = (AT)C::ld(G + 7 * pl + cp + 1, isg);
         }
 
-        /* momentsPre (deviations) */
-        float drho = 0.f, dT = 0.f;
-#pragma unroll
-        for (int k = 0; k < 9; k++) { drho += f[k]; dT += g[k]; }
-        const float rho = c.rho0 + drho;
-        const float irho = 1.0f / rho;
-        float u = irho * (f[1] - f[3] + f[5] - f[6] - f[7] + f[8]);
-        float v = irho * (f[2] - f[4] + f[5] + f[6] - f[7] - f[8]);
-        const float dT2 = dT, u2 = u, v2 = v;
+        node_lp<S, PT, AT, TANH, MOM>(s, c, x, y, cc, E, f, g, ap, am, pc);
 
-        /* phase_field (in PT) */
-        const PT one = (PT)1, half = (PT)0.5;
-        const PT th = tanh_pt<PT>(((PT)c.T0mTcrit_d + (PT)dT) * (PT)c.inv_T_width_d, TANH);
-        const PT kp = ap[1][1] + ap[1][2] + ap[2][1] + ap[1][0] + ap[0][1] + ap[2][2] + ap[2][0] + ap[0][0] + ap[0][2];
-        const PT km = am[1][1] + am[1][2] + am[2][1] + am[1][0] + am[0][1] + am[2][2] + am[2][0] + am[0][0] + am[0][2];
-        const PT p0 = pc[1];
-        const PT kpp = kp * (PT)0.125 * (half * (one + th));
-        const PT kmm = km * (PT)0.125 * (half * (one - th));
-        const PT phn_p = p0 + (half * kpp * (one - p0) - half * kmm * (one + p0));
-        const float phn = (float)phn_p;
-
-        /* forces: latent heat in FP64 */
-        dT = (float)((double)dT - c.dts * ((double)phn_p - (double)p0) * 0.5);
-        const float T = c.T0 + dT;
-        const float omp = 1.0f - phn;
-        const float forceY = rho * c.gb * T * (1.0f + 0.5f * phn) - 0.5f * v * omp;
-        const float forceX = -0.5f * u * omp;
-        const float iw = 1.0f / (c.omega_f * rho);
-        u = u + forceX * iw;
-        v = v + forceY * iw;
-
-        /* collision */
-        float Q[9], eq[9], out[9];
-        qpoly(u, v, Q);
-#pragma unroll
-        for (int k = 0; k < 9; k++) eq[k] = c.w[k] * (c.rho0 * Q[k] + drho * (1.0f + Q[k]));
-        reg_relax_lp(c, f, eq, c.cf, out);
-#pragma unroll
-        for (int k = 0; k < 9; k++) { C::st(s.fout + k * pl + cc, out[k], s.sf); f[k] = out[k]; }
-#pragma unroll
-        for (int k = 0; k < 9; k++) eq[k] = c.w[k] * (c.T0 * Q[k] + dT * (1.0f + Q[k]));
-        reg_relax_lp(c, g, eq, c.cg, out);
-#pragma unroll
-        for (int k = 0; k < 9; k++) C::st(s.gout + k * pl + cc, out[k], s.sg);
-        s.phout[cc] = phn_p;
-
-        if (MOM || E) {
-            float sg = 0.f;
-#pragma unroll
-            for (int k = 0; k < 9; k++) sg += out[k];
-            const double Tm = c.T0d + 0.5 * ((double)sg + (double)dT2);
-            if (E) s.tcout[y] = Tm;
-            if (MOM) {
-                float sf = 0.f;
-#pragma unroll
-                for (int k = 0; k < 9; k++) sf += f[k];
-                const float rm = c.rho0 + sf;
-                const float irm = 1.0f / rm;
-                const float tu = irm * (f[1] - f[3] + f[5] - f[6] - f[7] + f[8]);
-                const float tv = irm * (f[2] - f[4] + f[5] + f[6] - f[7] - f[8]);
-                const size_t q = (size_t)(x + 1) + (size_t)s.NX2 * (size_t)(y + 1);
-                s.mrho[q] = (double)c.rho0 + (double)sf;
-                s.mT[q] = Tm;
-                s.mu[q] = 0.5 * ((double)tu + (double)u2);
-                s.mv[q] = 0.5 * ((double)tv + (double)v2);
-                s.mphi[q] = (double)phn_p;
-            }
-        }
 #pragma unroll
         for (int k = 0; k < 3; k++) {
             ap[0][k] = ap[1][k]; ap[1][k] = ap[2][k];
@@ -325,6 +343,191 @@ fused_lowp_kernel(LpPtrs<S, PT> s, ConstsLP c, int H, int pf)
         }
         pc[0] = pc[1]; pc[1] = pc[2];
     }
+}
+
+/* The reduced-precision step on the shared-memory pipeline of
+ * fused_pipe.cuh: identical producer, consumers decode deviations from the
+ * stage and call node_lp. */
+template <typename S, typename PT, typename AT, int D, int TANH, bool MOM>
+__global__ void __launch_bounds__(PIPE_THREADS, 4)
+fused_pipe_lp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, PipeSched sch, int *errflag)
+{
+    using Gm = PipeGeom<S, PT>;
+    using C = Codec<S>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem);
+    uint64_t *empty = full + D;
+    unsigned char *stages = smem + Gm::HEADER;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int Nx = c.Nx, Ny = c.Ny;
+    if (tid == 0) {
+        for (int d = 0; d < D; d++) {
+            mbar_init(&full[d], 1);
+            mbar_init(&empty[d], PIPE_CWARPS);
+        }
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (warp == PIPE_CWARPS) {
+        if (lane != 0) return;
+        PipeIter it;
+        long long r = 0;
+        bool ok = it.start(sch, Ny);
+        while (ok) {
+            const int st = (int)(r % D);
+            if (r >= D && !mbar_wait(&empty[st], (uint32_t)(((r / D) - 1) & 1))) {
+                atomicExch(errflag, 1);
+                break;
+            }
+            pipe_issue<S, PT>(s.fin, s.gin, s.phin, s.plane, s.P, Ny, it.x0, it.y,
+                              stages + (size_t)st * Gm::STAGE_BYTES, &full[st]);
+            r++;
+            ok = it.next();
+        }
+        for (long long q = (r > D ? r - D : 0); q < r; q++)
+            if (!mbar_wait(&full[q % D], (uint32_t)((q / D) & 1))) atomicExch(errflag, 2);
+        return;
+    }
+    const long long pl = s.plane;
+    const int P = s.P;
+    const S *__restrict__ F = s.fin;
+    const PT *__restrict__ PH = s.phin;
+    const float isf = s.inv_sf, isg = s.inv_sg;
+    PipeIter it;
+    long long r = 0;
+    bool ok = it.start(sch, Ny);
+    while (ok) {
+        const int x = it.x0 + tid;
+        const bool active = x < Nx;
+        const bool W = (x == 0), E = (x == Nx - 1);
+        PT ap[3][3], am[3][3], pc[3];
+        const PT h = (PT)0.5, one = (PT)1;
+        if (active) {
+            for (int slot = 0; slot < 2; slot++) {
+                const int rr = it.y - 1 + slot;
+                const int rc = rr < 0 ? 0 : (rr >= Ny ? Ny - 1 : rr);
+                const PT *row = PH + (long long)rc * P;
+                const PT pL = W ? (PT)s.phiW[rc] : row[x - 1];
+                const PT pM = row[x];
+                const PT pR = E ? (PT)s.phiE[rc] : row[x + 1];
+                const PT a0 = h * (one + pL), a1 = h * (one + pM), a2 = h * (one + pR);
+                const PT b0 = h * (one - pL), b1 = h * (one - pM), b2 = h * (one - pR);
+                ap[slot][0] = a0 * a0; ap[slot][1] = a1 * a1; ap[slot][2] = a2 * a2;
+                am[slot][0] = b0 * b0; am[slot][1] = b1 * b1; am[slot][2] = b2 * b2;
+                pc[slot] = pM;
+            }
+        }
+        const int tile = it.t;
+        bool failed = false;
+        do {
+            const int y = it.y;
+            const int st = (int)(r % D);
+            if (!mbar_wait(&full[st], (uint32_t)((r / D) & 1))) {
+                atomicExch(errflag, 3);
+                failed = true;
+                break;
+            }
+            const S *sp = reinterpret_cast<const S *>(stages + (size_t)st * Gm::STAGE_BYTES);
+            const S *sg = sp + 9 * Gm::RW;
+            const PT *sphi = reinterpret_cast<const PT *>(stages + (size_t)st * Gm::STAGE_BYTES + 18 * Gm::POP_BYTES);
+            if (active) {
+                const bool Sb = (y == 0), N = (y == Ny - 1);
+                const long long cc = (long long)y * P + x;
+                const int col = tid + Gm::AL;
+                {
+                    const int rc = (y + 1 >= Ny) ? Ny - 1 : y + 1;
+                    const PT pL = W ? (PT)s.phiW[rc] : sphi[Gm::ALP + tid - 1];
+                    const PT pM = sphi[Gm::ALP + tid];
+                    const PT pR = E ? (PT)s.phiE[rc] : sphi[Gm::ALP + tid + 1];
+                    const PT a0 = h * (one + pL), a1 = h * (one + pM), a2 = h * (one + pR);
+                    const PT b0 = h * (one - pL), b1 = h * (one - pM), b2 = h * (one - pR);
+                    ap[2][0] = a0 * a0; ap[2][1] = a1 * a1; ap[2][2] = a2 * a2;
+                    am[2][0] = b0 * b0; am[2][1] = b1 * b1; am[2][2] = b2 * b2;
+                    pc[2] = pM;
+                }
+                AT f[9], g[9];
+                f[0] = (AT)C::ld(sp + 0 * Gm::RW + col, isf);
+                f[1] = (AT)C::ld(W ? sp + 3 * Gm::RW + col : sp + 1 * Gm::RW + col - 1, isf);
+                f[2] = (AT)C::ld(sp + 2 * Gm::RW + col, isf);
+                f[3] = (AT)C::ld(E ? sp + 1 * Gm::RW + col : sp + 3 * Gm::RW + col + 1, isf);
+                f[4] = (AT)C::ld(sp + 4 * Gm::RW + col, isf);
+                f[5] = (AT)C::ld(sp + 5 * Gm::RW + col - 1, isf);
+                f[6] = (AT)C::ld(sp + 6 * Gm::RW + col + 1, isf);
+                f[7] = (AT)C::ld(sp + 7 * Gm::RW + col + 1, isf);
+                f[8] = (AT)C::ld(sp + 8 * Gm::RW + col - 1, isf);
+                if (W || E || Sb || N) {
+                    if (Sb) f[2] = (AT)C::ld(F + 4 * pl + cc, isf);
+                    if (N) f[4] = (AT)C::ld(F + 2 * pl + cc, isf);
+                    if (W || Sb) f[5] = (AT)C::ld(F + 7 * pl + cc, isf);
+                    if (E || Sb) f[6] = (E && Sb) ? (AT)(s.corner[0] - c.w_d[6] * c.rho0d) : (AT)C::ld(F + 8 * pl + cc, isf);
+                    if (E || N) f[7] = (E && N) ? (AT)(s.corner[1] - c.w_d[7] * c.rho0d) : (AT)C::ld(F + 5 * pl + cc, isf);
+                    if (W || N) f[8] = (AT)C::ld(F + 6 * pl + cc, isf);
+                }
+                const int ym = Sb ? y : y - 1, yp = N ? y : y + 1;
+                g[0] = (AT)C::ld(sg + 0 * Gm::RW + col, isg);
+                g[2] = (AT)C::ld(sg + 2 * Gm::RW + col, isg);
+                g[4] = (AT)C::ld(sg + 4 * Gm::RW + col, isg);
+                if (W) {
+                    g[1] = (AT)(s.gW[y] - c.w_d[1] * c.T0d);
+                    g[5] = (AT)(s.gW[Ny + ym] - c.w_d[5] * c.T0d);
+                    g[8] = (AT)(s.gW[2 * Ny + yp] - c.w_d[8] * c.T0d);
+                } else {
+                    g[1] = (AT)C::ld(sg + 1 * Gm::RW + col - 1, isg);
+                    g[5] = (AT)C::ld(sg + 5 * Gm::RW + col - 1, isg);
+                    g[8] = (AT)C::ld(sg + 8 * Gm::RW + col - 1, isg);
+                }
+                if (E) {
+                    g[3] = (AT)(c.w_d[3] * s.tcin[y] * s.pE[y] - c.w_d[3] * c.T0d);
+                    g[6] = (AT)(c.w_d[6] * s.tcin[ym] * s.pE[Ny + ym] - c.w_d[6] * c.T0d);
+                    g[7] = (AT)(c.w_d[7] * s.tcin[yp] * s.pE[2 * Ny + yp] - c.w_d[7] * c.T0d);
+                } else {
+                    g[3] = (AT)C::ld(sg + 3 * Gm::RW + col + 1, isg);
+                    g[6] = (AT)C::ld(sg + 6 * Gm::RW + col + 1, isg);
+                    g[7] = (AT)C::ld(sg + 7 * Gm::RW + col + 1, isg);
+                }
+                node_lp<S, PT, AT, TANH, MOM>(s, c, x, y, cc, E, f, g, ap, am, pc);
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    ap[0][k] = ap[1][k]; ap[1][k] = ap[2][k];
+                    am[0][k] = am[1][k]; am[1][k] = am[2][k];
+                }
+                pc[0] = pc[1]; pc[1] = pc[2];
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[st]);
+            r++;
+            ok = it.next();
+        } while (ok && it.t == tile);
+        if (failed) break;
+    }
+}
+
+template <typename S, typename PT, typename AT, int D, int T, bool M>
+cudaError_t pipe_lp_launch(bgk_ctx *c, const LpPtrs<S, PT> &s, const ConstsLP<AT> &lp, int ctas)
+{
+    using Gm = PipeGeom<S, PT>;
+    const size_t smem = Gm::smem_bytes(D);
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(fused_pipe_lp_kernel<S, PT, AT, D, T, M>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    int grid;
+    const PipeSched sch = pipe_sched(c, ctas, &grid);
+    fused_pipe_lp_kernel<S, PT, AT, D, T, M><<<grid, PIPE_THREADS, smem, c->stream>>>(s, lp, sch, c->errflag);
+    return cudaGetLastError();
+}
+
+template <typename S, typename PT, typename AT, int D>
+cudaError_t pipe_lp_dispatch(bgk_ctx *c, const LpPtrs<S, PT> &s, const ConstsLP<AT> &lp, bool mom, int ctas)
+{
+    if (c->opt.tanh_mode == BGK_TANH_PORTABLE)
+        return mom ? pipe_lp_launch<S, PT, AT, D, BGK_TANH_PORTABLE, true>(c, s, lp, ctas)
+                   : pipe_lp_launch<S, PT, AT, D, BGK_TANH_PORTABLE, false>(c, s, lp, ctas);
+    return mom ? pipe_lp_launch<S, PT, AT, D, BGK_TANH_DEVICE, true>(c, s, lp, ctas)
+               : pipe_lp_launch<S, PT, AT, D, BGK_TANH_DEVICE, false>(c, s, lp, ctas);
 }
 
 /* Initial condition in deviation storage (STEP_7/initialization.f90 with
@@ -384,28 +587,29 @@ __global__ void lp_tcol_kernel(Consts c, const double *ref, double *tcol)
     if (j <= c.Ny) tcol[j - 1] = ref[(size_t)c.Nx + (size_t)(c.Nx + 2) * (size_t)j];
 }
 
-ConstsLP make_lp(const bgk_ctx *b)
+template <typename AT>
+ConstsLP<AT> make_lp(const bgk_ctx *b)
 {
     const Consts &c = b->c;
-    ConstsLP l{};
+    ConstsLP<AT> l{};
     l.Nx = c.Nx;
     l.Ny = c.Ny;
     for (int k = 0; k < 9; k++) {
-        l.w[k] = (float)c.w[k];
+        l.w[k] = (AT)c.w[k];
         l.w_d[k] = c.w[k];
-        l.cf[k] = (float)((1.0 - c.omega_f) * c.C[k]);
-        l.cg[k] = (float)((1.0 - c.omega_g) * c.C[k]);
+        l.cf[k] = (AT)((1.0 - c.omega_f) * c.C[k]);
+        l.cg[k] = (AT)((1.0 - c.omega_g) * c.C[k]);
     }
-    l.m = (float)c.m_cs2;
-    l.q = (float)c.q_cs2;
-    l.rho0 = (float)c.rho0;
-    l.T0 = (float)c.T0;
-    l.T0mTcrit = (float)(c.T0 - c.T_crit - c.T_act);
-    l.inv_T_width = (float)(1.0 / c.T_width);
-    l.f_plus = (float)c.f_plus;
-    l.f_minus = (float)c.f_minus;
-    l.gb = (float)(c.grav * c.beta);
-    l.omega_f = (float)c.omega_f;
+    l.m = (AT)c.m_cs2;
+    l.q = (AT)c.q_cs2;
+    l.rho0 = (AT)c.rho0;
+    l.T0 = (AT)c.T0;
+    l.T0mTcrit = (AT)(c.T0 - c.T_crit - c.T_act);
+    l.inv_T_width = (AT)(1.0 / c.T_width);
+    l.f_plus = (AT)c.f_plus;
+    l.f_minus = (AT)c.f_minus;
+    l.gb = (AT)(c.grav * c.beta);
+    l.omega_f = (AT)c.omega_f;
     l.dts = c.dts;
     l.T0mTcrit_d = c.T0 - c.T_crit - c.T_act;
     l.inv_T_width_d = 1.0 / c.T_width;
@@ -414,7 +618,7 @@ ConstsLP make_lp(const bgk_ctx *b)
     return l;
 }
 
-template <typename S, typename PT>
+template <typename S, typename PT, typename AT>
 cudaError_t launch_lowp_t(bgk_ctx *c, bool moments)
 {
     LpPtrs<S, PT> s{};
@@ -427,10 +631,18 @@ cudaError_t launch_lowp_t(bgk_ctx *c, bool moments)
     s.mrho = c->mrho; s.mT = c->mT; s.mu = c->mu; s.mv = c->mv; s.mphi = c->mphi;
     s.plane = c->plane; s.P = c->P; s.NX2 = c->NX2;
     s.sf = c->scale.sf; s.sg = c->scale.sg; s.inv_sf = c->scale.inv_sf; s.inv_sg = c->scale.inv_sg;
-    const ConstsLP lp = make_lp(c);
+    const ConstsLP<AT> lp = make_lp<AT>(c);
     const int H = strip_height(c);
     dim3 grd((c->Nx + FUSED_BX - 1) / FUSED_BX, (c->Ny + H - 1) / H);
-#define BGK_LP(T, M) fused_lowp_kernel<S, PT, T, M><<<grd, FUSED_BX, 0, c->stream>>>(s, lp, H, c->tune_pf)
+    if (c->tune_pipe) {
+        /* stages of ~11 KB (FP32) / ~6 KB (FP16): deeper rings, 4 CTAs per SM */
+        const int D = c->tune_D > 0 ? c->tune_D : 4;
+        const int ctas = c->tune_ctas > 0 ? c->tune_ctas : 4;
+        if (D <= 3) return pipe_lp_dispatch<S, PT, AT, 3>(c, s, lp, moments, ctas);
+        if (D >= 6) return pipe_lp_dispatch<S, PT, AT, 6>(c, s, lp, moments, ctas);
+        return pipe_lp_dispatch<S, PT, AT, 4>(c, s, lp, moments, ctas);
+    }
+#define BGK_LP(T, M) fused_lowp_kernel<S, PT, AT, T, M><<<grd, FUSED_BX, 0, c->stream>>>(s, lp, H, c->tune_pf)
     if (c->opt.tanh_mode == BGK_TANH_PORTABLE) {
         if (moments) BGK_LP(BGK_TANH_PORTABLE, true); else BGK_LP(BGK_TANH_PORTABLE, false);
     } else {
@@ -445,9 +657,11 @@ cudaError_t launch_lowp_t(bgk_ctx *c, bool moments)
 cudaError_t launch_fused_lowp(bgk_ctx *c, bool moments)
 {
     const bool p64 = c->phisz == 8;
-    if (c->opt.precision == BGK_PREC_F32)
-        return p64 ? launch_lowp_t<float, double>(c, moments) : launch_lowp_t<float, float>(c, moments);
-    return p64 ? launch_lowp_t<__half, double>(c, moments) : launch_lowp_t<__half, float>(c, moments);
+    if (c->opt.precision == BGK_PREC_F32) {
+        if (c->opt.fma == 2) return launch_lowp_t<float, double, double>(c, moments);   /* FP64 arithmetic */
+        return p64 ? launch_lowp_t<float, double, float>(c, moments) : launch_lowp_t<float, float, float>(c, moments);
+    }
+    return p64 ? launch_lowp_t<__half, double, float>(c, moments) : launch_lowp_t<__half, float, float>(c, moments);
 }
 
 /* FP16 scales: powers of two that put the largest deviations expected in
