@@ -29,6 +29,7 @@ UNITS = {
     "kernels_fast.cu": ["--fmad=true"],
     "capi.cu": ["--fmad=false"],
     "adjoint.cu": ["--fmad=true"],
+    "static_sums.cu": ["--fmad=false"],
 }
 
 

@@ -48,7 +48,10 @@ EXPORTS = [
     "bgk_phase_field", "bgk_forces", "bgk_collision", "bgk_moments", "bgk_upload",
     "bgk_download", "bgk_download_region", "bgk_field_sums", "bgk_get_it", "bgk_set_it",
     "bgk_set_tin", "bgk_sync", "bgk_get_stream", "bgk_save", "bgk_load", "bgk_adjoint_run",
+    "bgk_field_sums_static",
 ]
+
+STATIC_SUMS_MAX_NY = 32768
 
 
 class Params(ctypes.Structure):
@@ -123,6 +126,7 @@ def load() -> ctypes.CDLL:
         "bgk_save": (ctypes.c_int, [P, ctypes.c_char_p]),
         "bgk_load": (ctypes.c_int, [P, ctypes.c_char_p]),
         "bgk_adjoint_run": (ctypes.c_int, [P, ctypes.POINTER(AdjointSpec), dp, dp, dp]),
+        "bgk_field_sums_static": (ctypes.c_int, [P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P]),
     }
     for n in ("bgk_bc_f", "bgk_bc_g", "bgk_streaming", "bgk_moments_pre", "bgk_phase_field",
               "bgk_forces", "bgk_collision", "bgk_moments"):

@@ -202,6 +202,46 @@ typedef struct bgk_adjoint_spec {
 int bgk_adjoint_run(bgk_ctx *ctx, const bgk_adjoint_spec *spec, double *loss,
                     double *grad_tin, double *grad_tau_g);
 
+/* ---------------------------------------------------- allocation-free sums */
+/* Rows the static scratch of bgk_field_sums_static holds: 4 doubles per row,
+ * 1 MiB per device. */
+#define BGK_STATIC_SUMS_MAX_NY 32768
+
+/* The four sums of bgk_field_sums (STEP_7/field_check.f90:9-17,
+ * STEP_7/diag.f90:82-91) over fields the caller keeps in its own device
+ * memory, computed without allocating anything.  No reference counterpart:
+ * the reference sums its host arrays in place.
+ *
+ * For a caller that cannot allocate device memory mid-run: a host that owns
+ * its rho/T/phi arrays on the GPU and must not create a context (bgk_create
+ * allocates the whole step state) nor call cudaMalloc/cudaFree (cudaFree
+ * synchronizes the device, and a fixed device-memory budget may leave no
+ * room).  The scratch is a static __device__ array inside the library.
+ *
+ * rho, T, phi: device arrays of the current device in the reference layout
+ * (0:Nx+1, 0:Ny+1), i fastest, row j at offset j*ld; the interior
+ * i = 1..Nx, j = 1..Ny is summed.  out: 4 doubles of device memory, written
+ * asynchronously on `stream` (a cudaStream_t; NULL = the legacy default
+ * stream): out[0] = sum rho, out[1] = sum T, out[2] = sum phi,
+ * out[3] = #(phi > 0).  The call does not wait and does not check the sums
+ * for NaN or Inf.  Agrees with bgk_field_sums to rounding (another order of
+ * addition); deterministic for given Nx, Ny.
+ *
+ * Limits and rules:
+ *  - Ny > BGK_STATIC_SUMS_MAX_NY is rejected with BGK_ERR_ARG before any
+ *    device work.
+ *  - Nothing in the scratch has to start at zero: every slot a call reads is
+ *    written earlier by the same call.
+ *  - The first call on each device looks up the scratch address
+ *    (cudaGetSymbolAddress) and caches it; make that first call before any
+ *    stream capture begins.
+ *  - All calls on one device share the scratch.  Calls that can overlap in
+ *    time (on different streams, or from host threads without ordering
+ *    between them) race and return wrong sums; calls on one stream are
+ *    ordered and safe. */
+int bgk_field_sums_static(const double *rho, const double *T, const double *phi, int Nx, int Ny,
+                          int ld, void *stream, double *out);
+
 /* Complete binary snapshot (populations, phi, frozen boundary values, it)
  * -- unlike the reference's text dump (STEP_7/dump_out.f90:5-18), which omits
  * phi and phi_prec.  A snapshot restores into a context of the same size and
