@@ -86,16 +86,21 @@ struct ConstsLP {
 };
 
 template <typename S> struct Codec;
+/* ld: read-only global load (ld.global.nc) -- global memory only.
+ * lds: plain load, for the shared-memory stages of the pipeline kernel. */
 template <> struct Codec<float> {
     static __device__ __forceinline__ float ld(const float *p, float) { return __ldg(p); }
+    static __device__ __forceinline__ float lds(const float *p, float) { return *p; }
     static __device__ __forceinline__ void st(float *p, float v, float) { *p = v; }
 };
 template <> struct Codec<double> {
     static __device__ __forceinline__ float ld(const double *p, float) { return (float)__ldg(p); }
+    static __device__ __forceinline__ float lds(const double *p, float) { return (float)*p; }
     static __device__ __forceinline__ void st(double *p, float v, float) { *p = (double)v; }
 };
 template <> struct Codec<__half> {
     static __device__ __forceinline__ float ld(const __half *p, float inv) { return __half2float(__ldg(p)) * inv; }
+    static __device__ __forceinline__ float lds(const __half *p, float inv) { return __half2float(*p) * inv; }
     static __device__ __forceinline__ void st(__half *p, float v, float s) { *p = __float2half_rn(v * s); }
 };
 
@@ -446,15 +451,15 @@ fused_pipe_lp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, PipeSched sch, int *errfla
                     pc[2] = pM;
                 }
                 AT f[9], g[9];
-                f[0] = (AT)C::ld(sp + 0 * Gm::RW + col, isf);
-                f[1] = (AT)C::ld(W ? sp + 3 * Gm::RW + col : sp + 1 * Gm::RW + col - 1, isf);
-                f[2] = (AT)C::ld(sp + 2 * Gm::RW + col, isf);
-                f[3] = (AT)C::ld(E ? sp + 1 * Gm::RW + col : sp + 3 * Gm::RW + col + 1, isf);
-                f[4] = (AT)C::ld(sp + 4 * Gm::RW + col, isf);
-                f[5] = (AT)C::ld(sp + 5 * Gm::RW + col - 1, isf);
-                f[6] = (AT)C::ld(sp + 6 * Gm::RW + col + 1, isf);
-                f[7] = (AT)C::ld(sp + 7 * Gm::RW + col + 1, isf);
-                f[8] = (AT)C::ld(sp + 8 * Gm::RW + col - 1, isf);
+                f[0] = (AT)C::lds(sp + 0 * Gm::RW + col, isf);
+                f[1] = (AT)C::lds(W ? sp + 3 * Gm::RW + col : sp + 1 * Gm::RW + col - 1, isf);
+                f[2] = (AT)C::lds(sp + 2 * Gm::RW + col, isf);
+                f[3] = (AT)C::lds(E ? sp + 1 * Gm::RW + col : sp + 3 * Gm::RW + col + 1, isf);
+                f[4] = (AT)C::lds(sp + 4 * Gm::RW + col, isf);
+                f[5] = (AT)C::lds(sp + 5 * Gm::RW + col - 1, isf);
+                f[6] = (AT)C::lds(sp + 6 * Gm::RW + col + 1, isf);
+                f[7] = (AT)C::lds(sp + 7 * Gm::RW + col + 1, isf);
+                f[8] = (AT)C::lds(sp + 8 * Gm::RW + col - 1, isf);
                 if (W || E || Sb || N) {
                     if (Sb) f[2] = (AT)C::ld(F + 4 * pl + cc, isf);
                     if (N) f[4] = (AT)C::ld(F + 2 * pl + cc, isf);
@@ -464,26 +469,26 @@ fused_pipe_lp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, PipeSched sch, int *errfla
                     if (W || N) f[8] = (AT)C::ld(F + 6 * pl + cc, isf);
                 }
                 const int ym = Sb ? y : y - 1, yp = N ? y : y + 1;
-                g[0] = (AT)C::ld(sg + 0 * Gm::RW + col, isg);
-                g[2] = (AT)C::ld(sg + 2 * Gm::RW + col, isg);
-                g[4] = (AT)C::ld(sg + 4 * Gm::RW + col, isg);
+                g[0] = (AT)C::lds(sg + 0 * Gm::RW + col, isg);
+                g[2] = (AT)C::lds(sg + 2 * Gm::RW + col, isg);
+                g[4] = (AT)C::lds(sg + 4 * Gm::RW + col, isg);
                 if (W) {
                     g[1] = (AT)(s.gW[y] - c.w_d[1] * c.T0d);
                     g[5] = (AT)(s.gW[Ny + ym] - c.w_d[5] * c.T0d);
                     g[8] = (AT)(s.gW[2 * Ny + yp] - c.w_d[8] * c.T0d);
                 } else {
-                    g[1] = (AT)C::ld(sg + 1 * Gm::RW + col - 1, isg);
-                    g[5] = (AT)C::ld(sg + 5 * Gm::RW + col - 1, isg);
-                    g[8] = (AT)C::ld(sg + 8 * Gm::RW + col - 1, isg);
+                    g[1] = (AT)C::lds(sg + 1 * Gm::RW + col - 1, isg);
+                    g[5] = (AT)C::lds(sg + 5 * Gm::RW + col - 1, isg);
+                    g[8] = (AT)C::lds(sg + 8 * Gm::RW + col - 1, isg);
                 }
                 if (E) {
                     g[3] = (AT)(c.w_d[3] * s.tcin[y] * s.pE[y] - c.w_d[3] * c.T0d);
                     g[6] = (AT)(c.w_d[6] * s.tcin[ym] * s.pE[Ny + ym] - c.w_d[6] * c.T0d);
                     g[7] = (AT)(c.w_d[7] * s.tcin[yp] * s.pE[2 * Ny + yp] - c.w_d[7] * c.T0d);
                 } else {
-                    g[3] = (AT)C::ld(sg + 3 * Gm::RW + col + 1, isg);
-                    g[6] = (AT)C::ld(sg + 6 * Gm::RW + col + 1, isg);
-                    g[7] = (AT)C::ld(sg + 7 * Gm::RW + col + 1, isg);
+                    g[3] = (AT)C::lds(sg + 3 * Gm::RW + col + 1, isg);
+                    g[6] = (AT)C::lds(sg + 6 * Gm::RW + col + 1, isg);
+                    g[7] = (AT)C::lds(sg + 7 * Gm::RW + col + 1, isg);
                 }
                 node_lp<S, PT, AT, TANH, MOM>(s, c, x, y, cc, E, f, g, ap, am, pc);
 #pragma unroll

@@ -59,8 +59,11 @@ def adjoint(p, tin, steps, pi, pj, target, checkpoint_every=45):
     return out
 
 
-def fd_check(p, tin, steps, pi, pj, target, grad_tin, grad_tau, ndir=16, h=1e-6, seed=1):
-    """Central differences along random unit directions in (Tin, tau_g)."""
+def fd_check(p, tin, steps, pi, pj, target, grad_tin, grad_tau, ndir=16, h=1e-3, seed=1):
+    """Central differences along random unit directions in (Tin, tau_g).
+
+    h is absolute.  Much smaller steps than 1e-3 drown the loss difference in
+    the rounding of the forward runs (Tin ~ 283 K)."""
     rng = np.random.default_rng(seed)
     rows = []
     for _ in range(ndir):

@@ -65,13 +65,20 @@ def test_adjoint_requires_smooth(lib):
 @pytest.mark.slow
 def test_adjoint_config4_fd_16_directions(lib):
     """512x512, Ra 1e5, 2000 steps, 64 probes, checkpoints every 45 steps:
-    relative error <= 1e-5 against central differences (h = 1e-6) on 16
-    random directions, and the gradient costs <= 4 forward solves."""
+    relative error <= 1e-5 against central differences on 16 random unit
+    directions in (Tin, tau_g), and the gradient costs <= 4 forward solves.
+
+    Step h = 1e-3 (kelvin along Tin; the same step along tau_g).  The
+    temperatures are ~283 K, so at h = 1e-6 the two perturbed losses differ
+    by ~1e-9 on a loss of ~1e-2 and the rounding of each forward run alone
+    gives the difference quotient 1e-6..1e-4 relative error.  The physics
+    varies on the scale of T_width = 10 K, so at h = 1e-3 the truncation
+    error of the central difference is ~(h / T_width)^2 = 1e-8."""
     from bgk_pcm_b200 import gradcheck as gc
     p, tin, tin_t, pi, pj = gc.setup()
     target = gc.forward_phi(p, tin_t, 2000, pi, pj)
     loss, g, gtau = gc.adjoint(p, tin, 2000, pi, pj, target, checkpoint_every=45)
-    rows = gc.fd_check(p, tin, 2000, pi, pj, target, g, gtau, ndir=16, h=1e-6)
+    rows = gc.fd_check(p, tin, 2000, pi, pj, target, g, gtau, ndir=16, h=1e-3)
     worst = max(r[2] for r in rows)
     print("adjoint config4: loss", loss, "worst rel err", worst)
     assert worst <= 1e-5, rows
