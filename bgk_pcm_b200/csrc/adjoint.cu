@@ -54,6 +54,8 @@ struct AdjPtrs {
     double *pout;                          /* Pi(n)                          */
     const double *gW, *pE, *phiW, *phiE, *corner;
     double *omg_acc;                       /* per-block running sums         */
+    const double *dgW;                     /* d gW_k / d Tin per row         */
+    double *gtin;                          /* dL/dTin per row                */
     long long plane;
     int P;
     int tanh_mode;
@@ -209,7 +211,24 @@ __device__ __forceinline__ double PI(const AdjPtrs &s, int k, int x, int y)
     return s.pin[k * s.plane + (long long)y * s.P + x];
 }
 
-__global__ void __launch_bounds__(AB_X *AB_Y)
+/* dL/dTin contributions of one step's pulled-g partials at row y (west
+ * column): pop 1 reads the west value of its own row, pop 5 that of row y-1
+ * (clamped), pop 8 that of row y+1 (clamped). */
+__device__ __forceinline__ double tin_partial(const double *pi, long long plane, int P, int Ny, const double *dgW,
+                                              int y)
+{
+    auto at = [&](int k, int yy) { return pi[(9 + k) * plane + (long long)yy * P]; };
+    double a = at(1, y) * dgW[y];
+    double b5 = 0.0, b8 = 0.0;
+    if (y + 1 < Ny) b5 += at(5, y + 1);
+    if (y == 0) b5 += at(5, 0);
+    if (y - 1 >= 0) b8 += at(8, y - 1);
+    if (y == Ny - 1) b8 += at(8, Ny - 1);
+    return a + b5 * dgW[Ny + y] + b8 * dgW[2 * Ny + y];
+}
+
+/* 2 blocks (16 warps) per SM: 128 registers, a few spilled words. */
+__global__ void __launch_bounds__(AB_X *AB_Y, 2)
 adj_step_kernel(AdjPtrs s, Consts c)
 {
     const int Nx = c.Nx, Ny = c.Ny;
@@ -257,6 +276,9 @@ adj_step_kernel(AdjPtrs s, Consts c)
                 if (dy == 1 && y == Ny - 1) { skp += PI(s, 18, xd, Ny - 1); skm += PI(s, 19, xd, Ny - 1); }
             }
         }
+        /* dL/dTin from Pi(n+1) (the partials of the later step), one
+         * thread per row, so the per-row sums keep a fixed order */
+        if (W) s.gtin[y] += tin_partial(s.pin, pl, P, Ny, s.dgW, y);
         const double ph = s.phi[cc];        /* phi_prec of step n */
         const double d0 = PI(s, 20, x, y);
         /* T(Nx, y) written by this (east) node: read by the east pulls of
@@ -339,22 +361,12 @@ adj_step_kernel(AdjPtrs s, Consts c)
     if (t == 0) s.omg_acc[blockIdx.y * gridDim.x + blockIdx.x] += red[0];
 }
 
-/* dL/dTin per row from the west nodes' pulled-g partials of one step:
- * pop 1 reads the west value of its own row, pop 5 that of row y-1
- * (clamped), pop 8 that of row y+1 (clamped). */
+/* dL/dTin per row from the west nodes' pulled-g partials of one step (the
+ * step kernel folds in those of the step after it; this kernel takes the
+ * partials of step 1 at the end of the sweep). */
 __global__ void adj_tin_kernel(const double *pi, long long plane, int P, int Ny, const double *dgW, double *grad)
 {
-    for (int y = threadIdx.x; y < Ny; y += blockDim.x) {
-        auto at = [&](int k, int yy) { return pi[(9 + k) * plane + (long long)yy * P]; };
-        double a = at(1, y) * dgW[y];
-        double b5 = 0.0, b8 = 0.0;
-        if (y + 1 < Ny) b5 += at(5, y + 1);
-        if (y == 0) b5 += at(5, 0);
-        if (y - 1 >= 0) b8 += at(8, y - 1);
-        if (y == Ny - 1) b8 += at(8, Ny - 1);
-        a += b5 * dgW[Ny + y] + b8 * dgW[2 * Ny + y];
-        grad[y] += a;
-    }
+    for (int y = threadIdx.x; y < Ny; y += blockDim.x) grad[y] += tin_partial(pi, plane, P, Ny, dgW, y);
 }
 
 /* d gW_k / d Tin = w_k * poly_k(u(0,j), v(0,j)) for k = 1, 5, 8 */
@@ -514,15 +526,16 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
             a.pin = pi[pin]; a.pout = pi[pin ^ 1];
             a.gW = c->gW; a.pE = c->pE; a.phiW = c->phiW; a.phiE = c->phiE; a.corner = c->corner;
             a.omg_acc = omg_acc;
+            a.dgW = dgW; a.gtin = gtin;
             a.plane = pl; a.P = c->P;
             a.tanh_mode = c->opt.tanh_mode;
             adj_step_kernel<<<grd, blk, 0, st>>>(a, c->c);
             ACK(cudaGetLastError());
-            adj_tin_kernel<<<1, 1024, 0, st>>>(pi[pin ^ 1], pl, c->P, Ny, dgW, gtin);
-            ACK(cudaGetLastError());
             pin ^= 1;
         }
     }
+    adj_tin_kernel<<<1, 1024, 0, st>>>(pi[pin], pl, c->P, Ny, dgW, gtin);
+    ACK(cudaGetLastError());
     adj_sum_kernel<<<1, 32, 0, st>>>(omg_acc, nblk, scal + 1);
     ACK(cudaGetLastError());
     double host[2];

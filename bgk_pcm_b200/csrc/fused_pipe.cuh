@@ -326,18 +326,27 @@ inline PipeSched pipe_sched(const bgk_ctx *c, int ctas_per_sm, int *grid)
     return sch;
 }
 
+/* Raise the kernel's dynamic shared-memory limit once per device (the
+ * attribute belongs to the device's context).  Devices past 63 set it on
+ * every launch. */
+template <typename K>
+inline cudaError_t pipe_configure(K kernel, size_t smem, int dev, std::atomic<unsigned long long> &done)
+{
+    const unsigned long long bit = (dev >= 0 && dev < 64) ? (1ull << dev) : 0ull;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+    const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_release);
+    return e;
+}
+
 template <int D, int T, bool M, bool R>
 inline cudaError_t pipe_f64_launch(const bgk_ctx *c, const StepPtrs<double> &s, int ctas)
 {
     using Gm = PipeGeom<double, double>;
     const size_t smem = Gm::smem_bytes(D);
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(fused_pipe_f64_kernel<D, T, M, R>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
+    static std::atomic<unsigned long long> done{0};
+    const cudaError_t e = pipe_configure(fused_pipe_f64_kernel<D, T, M, R>, smem, c->dev, done);
+    if (e != cudaSuccess) return e;
     int grid;
     const PipeSched sch = pipe_sched(c, ctas, &grid);
     fused_pipe_f64_kernel<D, T, M, R><<<grid, PIPE_THREADS, smem, c->stream>>>(s, c->c, c->corner, sch, c->errflag);

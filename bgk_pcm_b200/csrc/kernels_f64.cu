@@ -14,6 +14,8 @@
  *  - conversions between the compact state and the reference layout
  *  - field_sums_kernel      FP64 interior reductions (field_check / diag)
  */
+#include <atomic>
+
 #include "bgk_internal.h"
 #include "bgk_math.cuh"
 #include "../../include/bgk_portable_tanh.h"

@@ -7,6 +7,8 @@
  */
 #include <cuda_fp16.h>
 
+#include <atomic>
+
 #include "bgk_internal.h"
 #include "bgk_math.cuh"
 #include "../../include/bgk_portable_tanh.h"
@@ -512,13 +514,9 @@ cudaError_t pipe_lp_launch(bgk_ctx *c, const LpPtrs<S, PT> &s, const ConstsLP<AT
 {
     using Gm = PipeGeom<S, PT>;
     const size_t smem = Gm::smem_bytes(D);
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(fused_pipe_lp_kernel<S, PT, AT, D, T, M>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
+    static std::atomic<unsigned long long> done{0};
+    const cudaError_t e = pipe_configure(fused_pipe_lp_kernel<S, PT, AT, D, T, M>, smem, c->dev, done);
+    if (e != cudaSuccess) return e;
     int grid;
     const PipeSched sch = pipe_sched(c, ctas, &grid);
     fused_pipe_lp_kernel<S, PT, AT, D, T, M><<<grid, PIPE_THREADS, smem, c->stream>>>(s, lp, sch, c->errflag);
