@@ -310,14 +310,17 @@ fused_pipe_f64_kernel(StepPtrs<double> s, Consts c, const double *__restrict__ c
     }
 }
 
-inline PipeSched pipe_sched(const bgk_ctx *c, int ctas_per_sm, int *grid)
+/* Tile height: base_H rows (measured best on B200: 4 for FP64, 8 for the
+ * reduced-precision forms; taller tiles leave a partial last wave, shorter
+ * ones lose a little per tile), halved down to 1 while there are fewer than
+ * 4 tiles per resident CTA (small grids, e.g. 512^2 runs best at H = 1). */
+inline PipeSched pipe_sched(const bgk_ctx *c, int ctas_per_sm, int base_H, int *grid)
 {
     PipeSched sch;
     sch.nbands = (c->Nx + PIPE_BX - 1) / PIPE_BX;
     const long long slots = (long long)c->nsm * ctas_per_sm;
-    /* strips short enough for at least ~6 tiles per resident CTA */
-    int H = 64;
-    while (H > 8 && (long long)sch.nbands * ((c->Ny + H - 1) / H) < 6 * slots) H /= 2;
+    int H = base_H;
+    while (H > 1 && (long long)sch.nbands * ((c->Ny + H - 1) / H) < 4 * slots) H /= 2;
     if (c->tune_H > 0) H = c->tune_H;
     sch.H = H;
     sch.nstrips = (c->Ny + H - 1) / H;
@@ -348,7 +351,7 @@ inline cudaError_t pipe_f64_launch(const bgk_ctx *c, const StepPtrs<double> &s, 
     const cudaError_t e = pipe_configure(fused_pipe_f64_kernel<D, T, M, R>, smem, c->dev, done);
     if (e != cudaSuccess) return e;
     int grid;
-    const PipeSched sch = pipe_sched(c, ctas, &grid);
+    const PipeSched sch = pipe_sched(c, ctas, 4, &grid);
     fused_pipe_f64_kernel<D, T, M, R><<<grid, PIPE_THREADS, smem, c->stream>>>(s, c->c, c->corner, sch, c->errflag);
     return cudaGetLastError();
 }

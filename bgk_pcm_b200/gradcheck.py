@@ -59,23 +59,69 @@ def adjoint(p, tin, steps, pi, pj, target, checkpoint_every=45):
     return out
 
 
-def fd_check(p, tin, steps, pi, pj, target, grad_tin, grad_tau, ndir=16, h=1e-3, seed=1):
-    """Central differences along random unit directions in (Tin, tau_g).
+def fd_check(p, tin, steps, pi, pj, target, grad_tin, grad_tau, ndir=16, h=1e-6, seed=1, tin_unit=None):
+    """Central differences along random unit directions in (theta, tau_g).
 
-    h is absolute.  Much smaller steps than 1e-3 drown the loss difference in
-    the rounding of the forward runs (Tin ~ 283 K)."""
+    theta is the dimensionless hot-wall temperature of the workload
+    definition (hot wall 1, solid 0): Tin = T_in_sol + tin_unit * theta with
+    tin_unit = T0 - T_in_sol, so a step h in theta moves Tin by h * tin_unit
+    kelvin.  The derivative along v is tin_unit * <dL/dTin, v_theta> +
+    dL/dtau_g * v_tau."""
+    if tin_unit is None:
+        tin_unit = p["T0"] - p["T_in_sol"]
     rng = np.random.default_rng(seed)
     rows = []
     for _ in range(ndir):
         v = rng.standard_normal(p["Ny"] + 1)
         v /= np.linalg.norm(v)
         vt, vtau = v[:-1], v[-1]
-        lp = loss_of(p, tin + h * vt, steps, pi, pj, target, p["tau_g"] + h * vtau)
-        lm = loss_of(p, tin - h * vt, steps, pi, pj, target, p["tau_g"] - h * vtau)
+        lp = loss_of(p, tin + h * tin_unit * vt, steps, pi, pj, target, p["tau_g"] + h * vtau)
+        lm = loss_of(p, tin - h * tin_unit * vt, steps, pi, pj, target, p["tau_g"] - h * vtau)
         fd = (lp - lm) / (2 * h)
-        ad = float(grad_tin @ vt + grad_tau * vtau)
+        ad = float(tin_unit * (grad_tin @ vt) + grad_tau * vtau)
         rows.append((fd, ad, abs(fd - ad) / max(abs(ad), 1e-300)))
     return rows
+
+
+def _autograd_function():
+    import torch
+
+    class AdjointLoss(torch.autograd.Function):
+        """L(Tin, tau_g) of the workload; the backward pass returns the
+        gradient that bgk_adjoint_run computed (ctypes, no torch kernels)."""
+
+        @staticmethod
+        def forward(ctx, tin, tau_g, p, steps, pi, pj, target, K):
+            q = dict(p)
+            q["tau_g"] = float(tau_g.detach().cpu())
+            s = Solver(q, smooth=True)
+            try:
+                s.initialization()
+                s.set_tin(tin.detach().cpu().numpy().astype(np.float64))
+                loss, g, gtau = s.adjoint(steps, pi, pj, target, K)
+            finally:
+                s.close()
+            ctx.save_for_backward(torch.from_numpy(g), torch.tensor(gtau, dtype=torch.float64))
+            return torch.tensor(loss, dtype=torch.float64)
+
+        @staticmethod
+        def backward(ctx, gout):
+            g, gtau = ctx.saved_tensors
+            return gout * g, gout * gtau, None, None, None, None, None, None
+
+    return AdjointLoss
+
+
+def adjoint_autograd(p, tin, steps, pi, pj, target, checkpoint_every=45):
+    """loss, dL/dTin, dL/dtau_g through torch.autograd (the gradient-check
+    harness's wrapper of the C ABI)."""
+    import torch
+    fn = _autograd_function()
+    t = torch.tensor(np.asarray(tin, dtype=np.float64), requires_grad=True)
+    tau = torch.tensor(float(p["tau_g"]), dtype=torch.float64, requires_grad=True)
+    loss = fn.apply(t, tau, p, steps, pi, pj, target, checkpoint_every)
+    loss.backward()
+    return float(loss), t.grad.numpy().copy(), float(tau.grad)
 
 
 def cost_ratio(p, tin, steps, pi, pj, target, checkpoint_every=45, repeats=3):

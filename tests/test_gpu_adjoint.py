@@ -65,23 +65,30 @@ def test_adjoint_requires_smooth(lib):
 @pytest.mark.slow
 def test_adjoint_config4_fd_16_directions(lib):
     """512x512, Ra 1e5, 2000 steps, 64 probes, checkpoints every 45 steps:
-    relative error <= 1e-5 against central differences on 16 random unit
-    directions in (Tin, tau_g), and the gradient costs <= 4 forward solves.
-
-    Step h = 1e-3 (kelvin along Tin; the same step along tau_g).  The
-    temperatures are ~283 K, so at h = 1e-6 the two perturbed losses differ
-    by ~1e-9 on a loss of ~1e-2 and the rounding of each forward run alone
-    gives the difference quotient 1e-6..1e-4 relative error.  The physics
-    varies on the scale of T_width = 10 K, so at h = 1e-3 the truncation
-    error of the central difference is ~(h / T_width)^2 = 1e-8."""
+    relative error <= 1e-5 against central differences with h = 1e-6 on 16
+    random unit directions in (theta, tau_g), theta the dimensionless
+    hot-wall temperature (Tin = T_in_sol + (T0 - T_in_sol) theta), and the
+    gradient costs <= 4 forward solves.  The gradient is taken through the
+    torch.autograd wrapper of the C ABI."""
     from bgk_pcm_b200 import gradcheck as gc
     p, tin, tin_t, pi, pj = gc.setup()
     target = gc.forward_phi(p, tin_t, 2000, pi, pj)
-    loss, g, gtau = gc.adjoint(p, tin, 2000, pi, pj, target, checkpoint_every=45)
-    rows = gc.fd_check(p, tin, 2000, pi, pj, target, g, gtau, ndir=16, h=1e-3)
+    loss, g, gtau = gc.adjoint_autograd(p, tin, 2000, pi, pj, target, checkpoint_every=45)
+    rows = gc.fd_check(p, tin, 2000, pi, pj, target, g, gtau, ndir=16, h=1e-6)
     worst = max(r[2] for r in rows)
     print("adjoint config4: loss", loss, "worst rel err", worst)
     assert worst <= 1e-5, rows
     ratio, tf, ta = gc.cost_ratio(p, tin, 2000, pi, pj, target)
     print(f"adjoint/forward cost {ratio:.2f} (forward {tf*1e3:.1f} ms, adjoint {ta*1e3:.1f} ms)")
     assert ratio <= 4.0
+
+
+def test_autograd_wrapper_matches_c_abi(lib):
+    """The torch.autograd.Function returns exactly what bgk_adjoint_run returns."""
+    from bgk_pcm_b200 import gradcheck as gc
+    p, tin, tin_t, pi, pj = gc.setup(Nx=32, Ny=24, steps=20, nprobes=10, **SENSITIVE)
+    target = gc.forward_phi(p, tin_t, 20, pi, pj)
+    a = gc.adjoint(p, tin, 20, pi, pj, target, checkpoint_every=5)
+    b = gc.adjoint_autograd(p, tin, 20, pi, pj, target, checkpoint_every=5)
+    assert a[0] == b[0] and a[2] == b[2]
+    np.testing.assert_array_equal(a[1], b[1])
