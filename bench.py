@@ -193,6 +193,30 @@ def e2e_run(params, precision, steps, device, torch):
     return ms, h2d, d2h
 
 
+def adjoint_cost(torch, repeats=3):
+    """Cost of one adjoint gradient against one forward solve on the
+    differentiation workload (512^2, Ra 1e5, 2000 steps, 64 probes,
+    checkpoints every 45 steps).  Wall clock around synchronised calls, so
+    the adjoint's workspace allocation is included; best of `repeats`."""
+    from bgk_pcm_b200 import Solver, gradcheck as gc
+    p, tin, tin_t, pi, pj = gc.setup()
+    steps, K = p["iter"], 45
+    target = gc.forward_phi(p, tin_t, steps, pi, pj)
+    fw, ad = [], []
+    for _ in range(repeats):
+        s = Solver(p, smooth=True)
+        s.initialization(); s.set_tin(tin); s.sync()
+        t0 = time.perf_counter(); s.step(steps); s.sync(); fw.append(time.perf_counter() - t0)
+        s.close()
+        s = Solver(p, smooth=True)
+        s.initialization(); s.set_tin(tin); s.sync()
+        t0 = time.perf_counter(); loss, _, _ = s.adjoint(steps, pi, pj, target, K); ad.append(time.perf_counter() - t0)
+        s.close()
+    return {"workload": "cavity512_ra1e5_adjoint", "steps": steps, "checkpoint_every": K,
+            "forward_ms": min(fw) * 1e3, "adjoint_ms": min(ad) * 1e3, "ratio": min(ad) / min(fw),
+            "loss": loss, "timing": "wall clock, synchronised, best of %d" % repeats}
+
+
 def run_reference(args, params, wl):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -222,8 +246,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cavity2048_ra1e6")
     ap.add_argument("--precision", default="f64", choices=["f64", "f32", "f16"])
-    ap.add_argument("--forms", default="f64fma", help="extra forms timed beside the headline (comma list)")
+    ap.add_argument("--forms", default="f64fma,f32,f16", help="extra forms timed beside the headline (comma list)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward cost leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -302,7 +327,11 @@ def main():
         g = nodes * max(args.steps // 4, 100) / (fms / 1e3) / 1e9
         b = BYTES_PER_NODE[prec]
         forms[form] = {"glups": g, "hbm_gbs": g * b, "frac_of_measured_hbm": g * b / hbm,
-                       "bytes_per_node": b}
+                       "bytes_per_node": b, "speedup_vs_headline": g / (value / world)}
+
+    adjoint = None
+    if rank == 0 and world == 1 and not args.no_adjoint:
+        adjoint = adjoint_cost(torch)
 
     e2e = None
     if not args.no_e2e:
@@ -338,6 +367,7 @@ def main():
                          "frac": achieved / hbm, "traffic": traffic, "peak_kind": hbm_kind,
                          "bytes_per_node": bpn},
             "forms": forms,
+            "adjoint": adjoint,
             "clocks": clocks,
             "e2e": e2e,
             "cpu_baseline": cpu,

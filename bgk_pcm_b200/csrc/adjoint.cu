@@ -23,6 +23,7 @@
  * Forward states come from snapshots every K steps; each K-step segment is
  * recomputed with the fused kernel before it is reversed.
  */
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -35,6 +36,8 @@
 namespace {
 
 using bgk::Consts;
+
+#include "pipe_common.cuh"
 
 constexpr int NPI = 21;          /* partial planes: f[9], g[9], k+, k-, phi_prec */
 constexpr int AB_X = 64, AB_Y = 4;
@@ -89,7 +92,7 @@ __device__ __forceinline__ void eq_poly_grad(double u, double v, double *du, dou
  *      where the selector-term derivatives are taken at the new value phn
  *      (the value the next step's stencils read).
  * out: f_b, g_b (pulled), kp_b, km_b, p0_b, omg_b (d/d omega_g). */
-__device__ void node_vjp(const Consts &c, int tanh_mode, const double *f, const double *g, double kp, double km,
+__device__ __forceinline__ void node_vjp(const Consts &c, int tanh_mode, const double *f, const double *g, double kp, double km,
                          double p0, const double *Fo_b, const double *Go_b, double d0, double skp, double skm,
                          double Tm_b, double *f_b, double *g_b, double &kp_b, double &km_b, double &p0_b,
                          double &omg_b)
@@ -361,6 +364,330 @@ adj_step_kernel(AdjPtrs s, Consts c)
     if (t == 0) s.omg_acc[blockIdx.y * gridDim.x + blockIdx.x] += red[0];
 }
 
+/* ------------------------------------------------------------------------
+ * The reverse step on the shared-memory pipeline (default).  Same
+ * arithmetic as adj_step_kernel; the loads are decoupled from the
+ * ~200-register node VJP: one producer lane per CTA streams, for each row y
+ * of a 128-column tile, 40 row segments into a stage with bulk asynchronous
+ * copies (16 bytes of neighbours on each side of the band):
+ *    0..8   Pi_k(n+1)        row y + c_ky (clamped)   gather of lambda_f
+ *    9..17  Pi_(9+k)(n+1)    row y + c_ky (clamped)   gather of lambda_g
+ *   18, 19  Pi_k+, Pi_k-     row y + 1 (clamped)      3x3 gather window
+ *   20      Pi_phi_prec      row y
+ *   21..29  f_k(n-1)         row y - c_ky (clamped)   pulls
+ *   30..38  g_k(n-1)         row y - c_ky (clamped)
+ *   39      phi(n-1)         row y + 1 (clamped)      3x3 stencil window
+ * Consumers keep the rows y-1 and y of the two 3x3 windows in registers.
+ * Values that a boundary node needs outside the staged rows (bounce-back
+ * partials, the clamped halo rows, the east T column, the west Tin terms)
+ * are read from global memory, as in adj_step_kernel.
+ * ---------------------------------------------------------------------- */
+constexpr int ADJ_AL = 2;                                 /* 16 bytes of doubles */
+constexpr int ADJ_RW = PIPE_BX + 2 * ADJ_AL;
+constexpr int ADJ_SEG_BYTES = ADJ_RW * (int)sizeof(double);
+constexpr int ADJ_NSEG = 40;
+constexpr int ADJ_STAGE_BYTES = ADJ_NSEG * ADJ_SEG_BYTES;
+constexpr int ADJ_HEADER = 256;
+constexpr int ADJ_D = 2;                                  /* stages */
+constexpr int ADJ_CTAS = 2;                               /* CTAs per SM */
+constexpr size_t ADJ_SMEM = (size_t)ADJ_HEADER + (size_t)ADJ_D * ADJ_STAGE_BYTES;
+
+__host__ __device__ constexpr int cx_of(int k) { return (k == 1 || k == 5 || k == 8) ? 1 : ((k == 3 || k == 6 || k == 7) ? -1 : 0); }
+__host__ __device__ constexpr int cy_of(int k) { return (k == 2 || k == 5 || k == 6) ? 1 : ((k == 4 || k == 7 || k == 8) ? -1 : 0); }
+__host__ __device__ constexpr int opp_of(int k) { return k == 0 ? 0 : (k <= 4 ? (k + 1) % 4 + 1 : (k + 1) % 4 + 5); }
+static_assert(opp_of(1) == 3 && opp_of(2) == 4 && opp_of(3) == 1 && opp_of(4) == 2, "opposites");
+static_assert(opp_of(5) == 7 && opp_of(6) == 8 && opp_of(7) == 5 && opp_of(8) == 6, "opposites");
+
+__device__ __forceinline__ int clamp_row(int r, int Ny) { return r < 0 ? 0 : (r >= Ny ? Ny - 1 : r); }
+
+__device__ __forceinline__ double warp_total(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+/* Producer: the 40 row-segment copies of work item (x0, y). */
+__device__ __forceinline__ void adj_issue(const AdjPtrs &s, int Ny, int x0, int y, unsigned char *stage,
+                                          uint64_t *full)
+{
+    mbar_arrive_expect_tx(full, ADJ_STAGE_BYTES);
+    const long long pl = s.plane;
+    const int P = s.P;
+#pragma unroll 1
+    for (int k = 0; k < 9; k++) {
+        const long long o1 = (long long)clamp_row(y + cy_of(k), Ny) * P + x0 - ADJ_AL;
+        const long long o2 = (long long)clamp_row(y - cy_of(k), Ny) * P + x0 - ADJ_AL;
+        bulk_g2s(stage + k * ADJ_SEG_BYTES, s.pin + k * pl + o1, ADJ_SEG_BYTES, full);
+        bulk_g2s(stage + (9 + k) * ADJ_SEG_BYTES, s.pin + (9 + k) * pl + o1, ADJ_SEG_BYTES, full);
+        bulk_g2s(stage + (21 + k) * ADJ_SEG_BYTES, s.f + k * pl + o2, ADJ_SEG_BYTES, full);
+        bulk_g2s(stage + (30 + k) * ADJ_SEG_BYTES, s.g + k * pl + o2, ADJ_SEG_BYTES, full);
+    }
+    const long long op = (long long)clamp_row(y + 1, Ny) * P + x0 - ADJ_AL;
+    const long long oy = (long long)y * P + x0 - ADJ_AL;
+    bulk_g2s(stage + 18 * ADJ_SEG_BYTES, s.pin + 18 * pl + op, ADJ_SEG_BYTES, full);
+    bulk_g2s(stage + 19 * ADJ_SEG_BYTES, s.pin + 19 * pl + op, ADJ_SEG_BYTES, full);
+    bulk_g2s(stage + 20 * ADJ_SEG_BYTES, s.pin + 20 * pl + oy, ADJ_SEG_BYTES, full);
+    bulk_g2s(stage + 39 * ADJ_SEG_BYTES, s.phi + op, ADJ_SEG_BYTES, full);
+}
+
+/* Sum of a Pi row over columns x-1..x+1 inside the domain. */
+__device__ __forceinline__ double row3(const double *v, int i, bool hasL, bool hasR)
+{
+    return (hasL ? v[i - 1] : 0.0) + v[i] + (hasR ? v[i + 1] : 0.0);
+}
+
+__global__ void __launch_bounds__(PIPE_THREADS, ADJ_CTAS)
+adj_pipe_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem);
+    uint64_t *empty = full + ADJ_D;
+    unsigned char *stages = smem + ADJ_HEADER;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int Nx = c.Nx, Ny = c.Ny;
+    if (tid == 0) {
+        for (int d = 0; d < ADJ_D; d++) {
+            mbar_init(&full[d], 1);
+            mbar_init(&empty[d], PIPE_CWARPS);
+        }
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (warp == PIPE_CWARPS) {
+        if (lane != 0) return;
+        PipeIter it;
+        long long r = 0;
+        bool ok = it.start(sch, Ny);
+        while (ok) {
+            const int st = (int)(r % ADJ_D);
+            if (r >= ADJ_D && !mbar_wait(&empty[st], (uint32_t)(((r / ADJ_D) - 1) & 1))) {
+                atomicExch(errflag, 11);
+                break;
+            }
+            adj_issue(s, Ny, it.x0, it.y, stages + (size_t)st * ADJ_STAGE_BYTES, &full[st]);
+            r++;
+            ok = it.next();
+        }
+        /* do not retire while copies into this CTA's shared memory are in flight */
+        for (long long q = (r > ADJ_D ? r - ADJ_D : 0); q < r; q++)
+            if (!mbar_wait(&full[q % ADJ_D], (uint32_t)((q / ADJ_D) & 1))) atomicExch(errflag, 12);
+        return;
+    }
+
+    const long long pl = s.plane;
+    const int P = s.P;
+    const double *__restrict__ PIN = s.pin;
+    double omg_sum = 0.0;
+    PipeIter it;
+    long long r = 0;
+    bool ok = it.start(sch, Ny);
+    while (ok) {
+        const int x = it.x0 + tid;
+        const bool active = x < Nx;
+        const bool W = (x == 0), E = (x == Nx - 1);
+        const bool hasL = x > 0, hasR = x + 1 < Nx;
+        double ap[3][3], am[3][3], pc[3], rk[3], rm[3];
+        if (active) {
+#pragma unroll
+            for (int slot = 0; slot < 2; slot++) {
+                const int rr = it.y - 1 + slot;
+                const int rc = clamp_row(rr, Ny);
+                const double *row = s.phi + (long long)rc * P;
+                const double pL = W ? s.phiW[rc] : row[x - 1];
+                const double pM = row[x];
+                const double pR = E ? s.phiE[rc] : row[x + 1];
+                ap[slot][0] = bgk::aplus(pL); ap[slot][1] = bgk::aplus(pM); ap[slot][2] = bgk::aplus(pR);
+                am[slot][0] = bgk::aminus(pL); am[slot][1] = bgk::aminus(pM); am[slot][2] = bgk::aminus(pR);
+                pc[slot] = pM;
+                if (rr >= 0) {
+                    rk[slot] = row3(PIN + 18 * pl + (long long)rr * P, x, hasL, hasR);
+                    rm[slot] = row3(PIN + 19 * pl + (long long)rr * P, x, hasL, hasR);
+                } else {
+                    rk[slot] = 0.0;
+                    rm[slot] = 0.0;
+                }
+            }
+        }
+        const int tile = it.t;
+        bool failed = false;
+        do {
+            const int y = it.y;
+            const int st = (int)(r % ADJ_D);
+            if (!mbar_wait(&full[st], (uint32_t)((r / ADJ_D) & 1))) {
+                atomicExch(errflag, 13);
+                failed = true;
+                break;
+            }
+            const double *stg = reinterpret_cast<const double *>(stages + (size_t)st * ADJ_STAGE_BYTES);
+            if (active) {
+                const bool S = (y == 0), N = (y == Ny - 1);
+                const long long cc = (long long)y * P + x;
+                const int col = tid + ADJ_AL;
+                /* new row y+1 of both windows */
+                {
+                    const int rc = clamp_row(y + 1, Ny);
+                    const double *sph = stg + 39 * ADJ_RW;
+                    const double pL = W ? s.phiW[rc] : sph[col - 1];
+                    const double pM = sph[col];
+                    const double pR = E ? s.phiE[rc] : sph[col + 1];
+                    ap[2][0] = bgk::aplus(pL); ap[2][1] = bgk::aplus(pM); ap[2][2] = bgk::aplus(pR);
+                    am[2][0] = bgk::aminus(pL); am[2][1] = bgk::aminus(pM); am[2][2] = bgk::aminus(pR);
+                    pc[2] = pM;
+                    if (y + 1 < Ny) {
+                        rk[2] = row3(stg + 18 * ADJ_RW, col, hasL, hasR);
+                        rm[2] = row3(stg + 19 * ADJ_RW, col, hasL, hasR);
+                    } else {
+                        rk[2] = 0.0;
+                        rm[2] = 0.0;
+                    }
+                }
+
+                /* 1. the adjoint of S(n) at this node */
+                double lf[9], lg[9];
+#pragma unroll
+                for (int k = 0; k < 9; k++) {
+                    const int xd = x + cx_of(k), yd = y + cy_of(k);
+                    const bool xin = xd >= 0 && xd < Nx, yin = yd >= 0 && yd < Ny;
+                    if (xin && yin) {
+                        lf[k] = stg[k * ADJ_RW + col + cx_of(k)];
+                    } else {
+                        /* read by this node's own bounce-back of opp(k), except
+                         * the two frozen corners (pop 6 at (Nx,1), pop 7 at (Nx,Ny)) */
+                        const bool corner6 = (k == 8) && E && S;
+                        const bool corner7 = (k == 5) && E && N;
+                        lf[k] = (corner6 || corner7) ? 0.0 : PIN[opp_of(k) * pl + cc];
+                    }
+                    double a = 0.0;
+                    if (xin) {
+                        if (yin) a += stg[(9 + k) * ADJ_RW + col + cx_of(k)];
+                        if (cy_of(k) == 1 && S) a += PIN[(9 + k) * pl + xd];
+                        if (cy_of(k) == -1 && N) a += PIN[(9 + k) * pl + (long long)(Ny - 1) * P + xd];
+                    }
+                    lg[k] = a;
+                }
+                const double skp = rk[0] + rk[1] + rk[2] + (S ? rk[1] : 0.0) + (N ? rk[1] : 0.0);
+                const double skm = rm[0] + rm[1] + rm[2] + (S ? rm[1] : 0.0) + (N ? rm[1] : 0.0);
+                const double d0 = stg[20 * ADJ_RW + col];
+                double lT = 0.0;
+                if (E) {
+                    lT += PIN[(9 + 3) * pl + cc] * c.w[3] * s.pE[y];
+                    double a6 = 0.0, a7 = 0.0;
+                    if (y + 1 < Ny) a6 += PIN[(9 + 6) * pl + cc + P];
+                    if (y == 0) a6 += PIN[(9 + 6) * pl + x];
+                    if (y - 1 >= 0) a7 += PIN[(9 + 7) * pl + cc - P];
+                    if (y == Ny - 1) a7 += PIN[(9 + 7) * pl + (long long)(Ny - 1) * P + x];
+                    lT += a6 * c.w[6] * s.pE[Ny + y] + a7 * c.w[7] * s.pE[2 * Ny + y];
+                }
+                /* dL/dTin from Pi(n+1), one thread per row */
+                if (W) s.gtin[y] += tin_partial(PIN, pl, P, Ny, s.dgW, y);
+
+                /* 2. pulled inputs of step n from S(n-1), as the forward pipeline */
+                const double *sp = stg + 21 * ADJ_RW, *sg = stg + 30 * ADJ_RW;
+                const double *F = s.f;
+                double f[9], g[9];
+                f[0] = sp[0 * ADJ_RW + col];
+                f[1] = W ? sp[3 * ADJ_RW + col] : sp[1 * ADJ_RW + col - 1];
+                f[2] = sp[2 * ADJ_RW + col];
+                f[3] = E ? sp[1 * ADJ_RW + col] : sp[3 * ADJ_RW + col + 1];
+                f[4] = sp[4 * ADJ_RW + col];
+                f[5] = sp[5 * ADJ_RW + col - 1];
+                f[6] = sp[6 * ADJ_RW + col + 1];
+                f[7] = sp[7 * ADJ_RW + col + 1];
+                f[8] = sp[8 * ADJ_RW + col - 1];
+                if (W || E || S || N) {
+                    if (S) f[2] = F[4 * pl + cc];
+                    if (N) f[4] = F[2 * pl + cc];
+                    if (W || S) f[5] = F[7 * pl + cc];
+                    if (E || S) f[6] = (E && S) ? s.corner[0] : F[8 * pl + cc];
+                    if (E || N) f[7] = (E && N) ? s.corner[1] : F[5 * pl + cc];
+                    if (W || N) f[8] = F[6 * pl + cc];
+                }
+                const int ym = S ? y : y - 1, yp = N ? y : y + 1;
+                g[0] = sg[0 * ADJ_RW + col];
+                g[2] = sg[2 * ADJ_RW + col];
+                g[4] = sg[4 * ADJ_RW + col];
+                if (W) {
+                    g[1] = s.gW[y];
+                    g[5] = s.gW[Ny + ym];
+                    g[8] = s.gW[2 * Ny + yp];
+                } else {
+                    g[1] = sg[1 * ADJ_RW + col - 1];
+                    g[5] = sg[5 * ADJ_RW + col - 1];
+                    g[8] = sg[8 * ADJ_RW + col - 1];
+                }
+                if (E) {
+                    g[3] = c.w[3] * s.tcol[y] * s.pE[y];
+                    g[6] = c.w[6] * s.tcol[ym] * s.pE[Ny + ym];
+                    g[7] = c.w[7] * s.tcol[yp] * s.pE[2 * Ny + yp];
+                } else {
+                    g[3] = sg[3 * ADJ_RW + col + 1];
+                    g[6] = sg[6 * ADJ_RW + col + 1];
+                    g[7] = sg[7 * ADJ_RW + col + 1];
+                }
+                const double kp = ap[1][1] + ap[1][2] + ap[2][1] + ap[1][0] + ap[0][1] + ap[2][2] + ap[2][0] +
+                                  ap[0][0] + ap[0][2];
+                const double km = am[1][1] + am[1][2] + am[2][1] + am[1][0] + am[0][1] + am[2][2] + am[2][0] +
+                                  am[0][0] + am[0][2];
+
+                /* 3. vector-Jacobian product -> Pi(n) */
+                double fb[9], gbv[9], kpb, kmb, p0b, omg_b;
+                node_vjp(c, s.tanh_mode, f, g, kp, km, pc[1], lf, lg, d0, skp, skm, lT, fb, gbv, kpb, kmb, p0b,
+                         omg_b);
+                omg_sum += omg_b;
+#pragma unroll
+                for (int k = 0; k < 9; k++) {
+                    s.pout[k * pl + cc] = fb[k];
+                    s.pout[(9 + k) * pl + cc] = gbv[k];
+                }
+                s.pout[18 * pl + cc] = kpb;
+                s.pout[19 * pl + cc] = kmb;
+                s.pout[20 * pl + cc] = p0b;
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    ap[0][k] = ap[1][k]; ap[1][k] = ap[2][k];
+                    am[0][k] = am[1][k]; am[1][k] = am[2][k];
+                }
+                pc[0] = pc[1]; pc[1] = pc[2];
+                rk[0] = rk[1]; rk[1] = rk[2];
+                rm[0] = rm[1]; rm[1] = rm[2];
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[st]);
+            r++;
+            ok = it.next();
+        } while (ok && it.t == tile);
+        if (failed) break;
+    }
+    /* d/d omega_g: one running partial per consumer warp, in a fixed order */
+    omg_sum = warp_total(omg_sum);
+    if (lane == 0) s.omg_acc[blockIdx.x * PIPE_CWARPS + warp] += omg_sum;
+}
+
+/* Tile height for the reverse step: the H that minimises the waves of tiles
+ * times (H + 1), the 1 standing for the per-tile window prologue. */
+PipeSched adj_sched(const bgk_ctx *c, int *grid)
+{
+    PipeSched sch;
+    sch.nbands = (c->Nx + PIPE_BX - 1) / PIPE_BX;
+    const long long slots = (long long)c->nsm * ADJ_CTAS;
+    long long best = -1;
+    int bestH = 1;
+    for (int H = 1; H <= 64; H++) {
+        const long long tiles = (long long)sch.nbands * ((c->Ny + H - 1) / H);
+        const long long waves = (tiles + slots - 1) / slots;
+        const long long cost = waves * (H + 1);
+        if (best < 0 || cost < best) { best = cost; bestH = H; }
+        if (H >= c->Ny) break;
+    }
+    if (c->tune_H > 0) bestH = c->tune_H;
+    sch.H = bestH;
+    sch.nstrips = (c->Ny + bestH - 1) / bestH;
+    sch.ntiles = sch.nbands * sch.nstrips;
+    *grid = (int)(sch.ntiles < slots ? sch.ntiles : slots);
+    return sch;
+}
+
 /* dL/dTin per row from the west nodes' pulled-g partials of one step (the
  * step kernel folds in those of the step after it; this kernel takes the
  * partials of step 1 at the end of the sweep). */
@@ -451,9 +778,16 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
     double *seg_raw = dmalloc((size_t)(K + 1) * state_elems * sizeof(double));
     double *snaps = snaps_raw ? snaps_raw + state_guard : nullptr;   /* state i at snaps + i*state_elems */
     double *seg = seg_raw ? seg_raw + state_guard : nullptr;
-    double *pi[2] = {dmalloc((size_t)NPI * pl * sizeof(double)), dmalloc((size_t)NPI * pl * sizeof(double))};
+    /* partial planes Pi, guarded like the states (the pipelined reverse step
+     * copies row segments of them) */
+    double *pi_raw[2] = {dmalloc(((size_t)NPI * pl + 2 * state_guard) * sizeof(double)),
+                         dmalloc(((size_t)NPI * pl + 2 * state_guard) * sizeof(double))};
+    double *pi[2] = {pi_raw[0] ? pi_raw[0] + state_guard : nullptr, pi_raw[1] ? pi_raw[1] + state_guard : nullptr};
+    const bool use_pipe = c->tune_pipe != 0;
     dim3 blk(AB_X, AB_Y), grd((c->Nx + AB_X - 1) / AB_X, (Ny + AB_Y - 1) / AB_Y);
-    const int nblk = grd.x * grd.y;
+    int pgrid = 0;
+    const PipeSched psch = adj_sched(c, &pgrid);
+    const int nblk = use_pipe ? pgrid * PIPE_CWARPS : (int)(grd.x * grd.y);
     double *omg_acc = dmalloc((size_t)nblk * sizeof(double));
     double *dgW = dmalloc(3 * (size_t)Ny * sizeof(double));
     double *gtin = dmalloc((size_t)Ny * sizeof(double));
@@ -483,6 +817,10 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
         return cudaMemcpyAsync(dst + 19 * pl, c->tcol[buf], Ny * sizeof(double), cudaMemcpyDeviceToDevice, st);
     };
 
+    if (use_pipe) {
+        static std::atomic<unsigned long long> done{0};
+        ACK(pipe_configure(adj_pipe_kernel, ADJ_SMEM, c->dev, done));
+    }
     ACK(cudaMemcpyAsync(dpi, spec->probe_i, spec->nprobes * sizeof(int), cudaMemcpyHostToDevice, st));
     ACK(cudaMemcpyAsync(dpj, spec->probe_j, spec->nprobes * sizeof(int), cudaMemcpyHostToDevice, st));
     ACK(cudaMemcpyAsync(dtg, spec->phi_target, spec->nprobes * sizeof(double), cudaMemcpyHostToDevice, st));
@@ -529,7 +867,10 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
             a.dgW = dgW; a.gtin = gtin;
             a.plane = pl; a.P = c->P;
             a.tanh_mode = c->opt.tanh_mode;
-            adj_step_kernel<<<grd, blk, 0, st>>>(a, c->c);
+            if (use_pipe)
+                adj_pipe_kernel<<<pgrid, PIPE_THREADS, ADJ_SMEM, st>>>(a, c->c, psch, c->errflag);
+            else
+                adj_step_kernel<<<grd, blk, 0, st>>>(a, c->c);
             ACK(cudaGetLastError());
             pin ^= 1;
         }
