@@ -882,7 +882,16 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
     double host[2];
     ACK(cudaMemcpyAsync(host, scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
     if (grad_tin) ACK(cudaMemcpyAsync(grad_tin, gtin, (size_t)Ny * sizeof(double), cudaMemcpyDeviceToHost, st));
+    int flag = 0;
+    ACK(cudaMemcpyAsync(&flag, c->errflag, sizeof(int), cudaMemcpyDeviceToHost, st));
     ACK(cudaStreamSynchronize(st));
+    if (flag) {
+        cudaMemsetAsync(c->errflag, 0, sizeof(int), st);
+        cudaStreamSynchronize(st);
+        cleanup();
+        return bgk_internal_fail(BGK_ERR_CUDA, "a bounded wait inside an adjoint or step kernel gave up; "
+                                               "the gradient is invalid");
+    }
     *loss = host[0];
     /* omega_g = 1/tau_g */
     const double tau_g = c->p.tau_g;
