@@ -134,3 +134,32 @@ def cost_ratio(p, tin, steps, pi, pj, target, checkpoint_every=45, repeats=3):
         t0 = time.perf_counter(); s.adjoint(steps, pi, pj, target, checkpoint_every); ad.append(time.perf_counter() - t0)
         s.close()
     return min(ad) / min(fw), min(fw), min(ad)
+
+
+def main(argv=None):
+    """python -m bgk_pcm_b200.gradcheck [adjoint|cost|fd]: one adjoint
+    gradient, the adjoint/forward cost, or the finite-difference check on
+    the differentiation workload."""
+    import argparse
+    import json
+    ap = argparse.ArgumentParser()
+    ap.add_argument("what", choices=["adjoint", "cost", "fd"])
+    ap.add_argument("--ndir", type=int, default=16)
+    a = ap.parse_args(argv)
+    p, tin, tin_t, pi, pj = setup()
+    steps = p["iter"]
+    target = forward_phi(p, tin_t, steps, pi, pj)
+    if a.what == "adjoint":
+        loss, g, gtau = adjoint(p, tin, steps, pi, pj, target)
+        print(json.dumps({"loss": loss, "grad_tau_g": gtau, "grad_tin_norm": float(np.linalg.norm(g))}))
+    elif a.what == "cost":
+        ratio, tf, ta = cost_ratio(p, tin, steps, pi, pj, target)
+        print(json.dumps({"ratio": ratio, "forward_ms": tf * 1e3, "adjoint_ms": ta * 1e3}))
+    else:
+        loss, g, gtau = adjoint_autograd(p, tin, steps, pi, pj, target)
+        rows = fd_check(p, tin, steps, pi, pj, target, g, gtau, ndir=a.ndir)
+        print(json.dumps({"loss": loss, "worst_rel_err": max(r[2] for r in rows), "rows": rows}))
+
+
+if __name__ == "__main__":
+    main()
