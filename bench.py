@@ -38,8 +38,9 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "GLUPS & HBM GB/s: FP32-store vs FP64 at ≤1e-4 err; adjoint/forward cost"
 # algorithmic bytes per node and step: 18 populations + phi, read once and
-# written once (FP64; FP32/FP16 deviations with phi kept in FP64)
-BYTES_PER_NODE = {"f64": 304, "f32": 160, "f16": 88}
+# written once (FP64; FP32 and FP16 deviations with phi in FP32; FP32
+# deviations with FP64 arithmetic and phi in FP64)
+BYTES_PER_NODE = {"f64": 304, "f32": 152, "f16": 80, "f32x": 160}
 FALLBACK_HBM = 6650.0
 
 
@@ -245,8 +246,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=100)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cavity2048_ra1e6")
-    ap.add_argument("--precision", default="f64", choices=["f64", "f32", "f16"])
-    ap.add_argument("--forms", default="f64fma,f32,f16", help="extra forms timed beside the headline (comma list)")
+    ap.add_argument("--precision", default="f64", choices=["f64", "f32", "f16", "f32x"])
+    ap.add_argument("--forms", default="f64fma,f32,f16,f32x", help="extra forms timed beside the headline (comma list)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward cost leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
@@ -361,7 +362,7 @@ def main():
             "config": {"workload": args.workload, "Nx": Nx, "Ny": Ny, "Ra": wl["Ra"], "Pr": wl["Pr"],
                        "Ste": wl["Ste"], "precision": args.precision, "parallelism": f"replicas{world}",
                        "l2": "inputs larger than L2 (A/B populations %.0f MB > 126 MB)"
-                             % (2 * 18 * {"f64": 8, "f32": 4, "f16": 2}[args.precision] * nodes / 1e6)},
+                             % (2 * 18 * {"f64": 8, "f32": 4, "f16": 2, "f32x": 4}[args.precision] * nodes / 1e6)},
             "hbm_gbs": value / world * bpn,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic, "peak_kind": hbm_kind,

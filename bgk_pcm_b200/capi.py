@@ -24,7 +24,7 @@ ERRORS = {
     -7: "BGK_ERR_NONFINITE",
 }
 
-PREC_F64, PREC_F32, PREC_F16 = 0, 1, 2
+PREC_F64, PREC_F32, PREC_F16, PREC_F32X = 0, 1, 2, 3
 TANH_DEVICE, TANH_PORTABLE = 0, 1
 
 FIELD_F0, FIELD_G0 = 0, 9

@@ -69,6 +69,20 @@ __device__ __forceinline__ double tanh_sel(double x, int mode)
     return mode == BGK_TANH_PORTABLE ? bgk_portable_tanh(x) : tanh(x);
 }
 
+__host__ __device__ constexpr int cx_of(int k) { return (k == 1 || k == 5 || k == 8) ? 1 : ((k == 3 || k == 6 || k == 7) ? -1 : 0); }
+__host__ __device__ constexpr int cy_of(int k) { return (k == 2 || k == 5 || k == 6) ? 1 : ((k == 4 || k == 7 || k == 8) ? -1 : 0); }
+
+/* The equilibrium polynomial P_k(u, v) = 1 + 3 c_k.u + 4.5 (c_k.u)^2 -
+ * 1.5 |u|^2 (same value as eq_poly up to rounding) and its gradient. */
+__device__ __forceinline__ double poly_k(int k, double u, double v, double &du, double &dv)
+{
+    const double cx = cx_of(k), cy = cy_of(k);
+    const double cu = cx * u + cy * v;
+    du = 3.0 * cx + 9.0 * cu * cx - 3.0 * u;
+    dv = 3.0 * cy + 9.0 * cu * cy - 3.0 * v;
+    return 1.0 + 3.0 * cu + 4.5 * cu * cu - 1.5 * (u * u + v * v);
+}
+
 /* dP_k/du and dP_k/dv of the equilibrium polynomials (see eq_poly). */
 __device__ __forceinline__ void eq_poly_grad(double u, double v, double *du, double *dv)
 {
@@ -92,9 +106,10 @@ __device__ __forceinline__ void eq_poly_grad(double u, double v, double *du, dou
  *      where the selector-term derivatives are taken at the new value phn
  *      (the value the next step's stencils read).
  * out: f_b, g_b (pulled), kp_b, km_b, p0_b, omg_b (d/d omega_g). */
+template <class FOB, class GOB, class OUTF, class OUTG>
 __device__ __forceinline__ void node_vjp(const Consts &c, int tanh_mode, const double *f, const double *g, double kp, double km,
-                         double p0, const double *Fo_b, const double *Go_b, double d0, double skp, double skm,
-                         double Tm_b, double *f_b, double *g_b, double &kp_b, double &km_b, double &p0_b,
+                         double p0, FOB Fo_b, GOB Go_b, double d0, double skp, double skm,
+                         double Tm_b, OUTF out_fb, OUTG out_gb, double &kp_b, double &km_b, double &p0_b,
                          double &omg_b)
 {
     const double m = c.m_cs2, q = c.q_cs2;
@@ -121,36 +136,33 @@ __device__ __forceinline__ void node_vjp(const Consts &c, int tanh_mode, const d
     const double FY = FY0 - v * omp * 0.5;
     const double orho = c.omega_f * rho;
     const double uf = u + FX / orho, vf = v + FY / orho;
-    double Pq[9], dPu[9], dPv[9];
-    bgk::eq_poly(uf, vf, Pq);
-    eq_poly_grad(uf, vf, dPu, dPv);
-    double e[9];
-#pragma unroll
-    for (int k = 0; k < 9; k++) e[k] = g[k] - c.w[k] * Tf * Pq[k];
+    /* non-equilibrium moments of g; the polynomials P_k(uf, vf) and their
+     * gradients are formed per k where they are used (fewer live registers) */
     double txx = 0.0, tyy = 0.0, txy = 0.0;
 #pragma unroll
     for (int k = 0; k < 9; k++) {
-        txx += (d_AisQ[k] ? q : m) * e[k];
-        tyy += (d_BisQ[k] ? q : m) * e[k];
-        txy += d_E[k] * e[k];
+        double du, dv;
+        const double e = g[k] - c.w[k] * Tf * poly_k(k, uf, vf, du, dv);
+        txx += (d_AisQ[k] ? q : m) * e;
+        tyy += (d_BisQ[k] ? q : m) * e;
+        txy += d_E[k] * e;
     }
 
     /* ---- reverse ---- */
-    double Gob[9];
-#pragma unroll
-    for (int k = 0; k < 9; k++) Gob[k] = Go_b[k] + 0.5 * Tm_b;
-    /* g collision: go_k = geq_k + (1-omega_g) C_k Sg_k */
+    const double hT = 0.5 * Tm_b;      /* moments T = (sum g + T2) / 2 */
+    /* g collision: go_k = geq_k + (1-omega_g) C_k Sg_k; f likewise */
     const double cg = 1.0 - c.omega_g, cf = 1.0 - c.omega_f;
     double txxb = 0.0, tyyb = 0.0, txyb = 0.0, pxxb = 0.0, pyyb = 0.0, pxyb = 0.0;
     omg_b = 0.0;
 #pragma unroll
     for (int k = 0; k < 9; k++) {
         const double A = d_AisQ[k] ? q : m, B = d_BisQ[k] ? q : m;
+        const double Gob = Go_b(k) + hT;
         const double Sg = A * txx + B * tyy + 2.0 * d_E[k] * txy;
-        omg_b += Gob[k] * (-c.C[k] * Sg);
-        const double sb = Gob[k] * cg * c.C[k];
+        omg_b += Gob * (-c.C[k] * Sg);
+        const double sb = Gob * cg * c.C[k];
         txxb += sb * A; tyyb += sb * B; txyb += 2.0 * sb * d_E[k];
-        const double sf = Fo_b[k] * cf * c.C[k];
+        const double sf = Fo_b(k) * cf * c.C[k];
         pxxb += sf * A; pyyb += sf * B; pxyb += 2.0 * sf * d_E[k];
     }
     double rhob = 0.0, Tfb = 0.0, ufb = 0.0, vfb = 0.0;
@@ -159,15 +171,15 @@ __device__ __forceinline__ void node_vjp(const Consts &c, int tanh_mode, const d
         const double A = d_AisQ[j] ? q : m, B = d_BisQ[j] ? q : m;
         const double eb = A * txxb + B * tyyb + d_E[j] * txyb;
         const double db = A * pxxb + B * pyyb + d_E[j] * pxyb;
-        g_b[j] = eb;
-        f_b[j] = db;
-        const double geqb = Gob[j] - eb;
-        const double feqb = Fo_b[j] - db;
-        rhob += feqb * c.w[j] * Pq[j];
-        Tfb += geqb * c.w[j] * Pq[j];
+        const double geqb = (Go_b(j) + hT) - eb;
+        const double feqb = Fo_b(j) - db;
+        double du, dv;
+        const double Pj = poly_k(j, uf, vf, du, dv);
+        rhob += feqb * c.w[j] * Pj;
+        Tfb += geqb * c.w[j] * Pj;
         const double Pb = c.w[j] * (feqb * rho + geqb * Tf);
-        ufb += Pb * dPu[j];
-        vfb += Pb * dPv[j];
+        ufb += Pb * du;
+        vfb += Pb * dv;
     }
     /* velocity shift */
     double ub = ufb, vb = vfb;
@@ -197,15 +209,20 @@ __device__ __forceinline__ void node_vjp(const Consts &c, int tanh_mode, const d
     const double rpb = KPb * kp / 8.0, rmb = KMb * km / 8.0;
     const double thb = 0.5 * rpb - 0.5 * rmb;
     Tb += thb * (1.0 - th * th) / c.T_width;
-    Tb += 0.5 * Tm_b;
+    Tb += hT;
     /* momentsPre */
     const double mxb = ub * irho, myb = vb * irho;
     const double irhob = ub * mx + vb * my;
     rhob += -irhob * irho * irho;
+    /* pulled-population adjoints: the collision term (recomputed from the
+     * six moment adjoints) plus the moment terms */
 #pragma unroll
     for (int j = 0; j < 9; j++) {
-        f_b[j] += rhob + d_cx[j] * mxb + d_cy[j] * myb;
-        g_b[j] += Tb;
+        const double A = d_AisQ[j] ? q : m, B = d_BisQ[j] ? q : m;
+        const double eb = A * txxb + B * tyyb + d_E[j] * txyb;
+        const double db = A * pxxb + B * pyyb + d_E[j] * pxyb;
+        out_fb(j, db + (rhob + cx_of(j) * mxb + cy_of(j) * myb));
+        out_gb(j, eb + Tb);
     }
 }
 
@@ -342,7 +359,9 @@ adj_step_kernel(AdjPtrs s, Consts c)
 
         /* 3. vector-Jacobian product -> Pi(n) */
         double fb[9], gbv[9], kpb, kmb, p0b;
-        node_vjp(c, s.tanh_mode, f, g, kp, km, ph, lf, lg, d0, skp, skm, lT, fb, gbv, kpb, kmb, p0b, omg_b);
+        node_vjp(c, s.tanh_mode, f, g, kp, km, ph, [&](int k) { return lf[k]; }, [&](int k) { return lg[k]; }, d0,
+                 skp, skm, lT, [&](int k, double v) { fb[k] = v; }, [&](int k, double v) { gbv[k] = v; }, kpb, kmb,
+                 p0b, omg_b);
 #pragma unroll
         for (int k = 0; k < 9; k++) {
             s.pout[k * pl + cc] = fb[k];
@@ -392,8 +411,6 @@ constexpr int ADJ_D = 2;                                  /* stages */
 constexpr int ADJ_CTAS = 2;                               /* CTAs per SM */
 constexpr size_t ADJ_SMEM = (size_t)ADJ_HEADER + (size_t)ADJ_D * ADJ_STAGE_BYTES;
 
-__host__ __device__ constexpr int cx_of(int k) { return (k == 1 || k == 5 || k == 8) ? 1 : ((k == 3 || k == 6 || k == 7) ? -1 : 0); }
-__host__ __device__ constexpr int cy_of(int k) { return (k == 2 || k == 5 || k == 6) ? 1 : ((k == 4 || k == 7 || k == 8) ? -1 : 0); }
 __host__ __device__ constexpr int opp_of(int k) { return k == 0 ? 0 : (k <= 4 ? (k + 1) % 4 + 1 : (k + 1) % 4 + 5); }
 static_assert(opp_of(1) == 3 && opp_of(2) == 4 && opp_of(3) == 1 && opp_of(4) == 2, "opposites");
 static_assert(opp_of(5) == 7 && opp_of(6) == 8 && opp_of(7) == 5 && opp_of(8) == 6, "opposites");
@@ -487,19 +504,18 @@ adj_pipe_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
         const bool active = x < Nx;
         const bool W = (x == 0), E = (x == Nx - 1);
         const bool hasL = x > 0, hasR = x + 1 < Nx;
-        double ap[3][3], am[3][3], pc[3], rk[3], rm[3];
+        /* windows: phi of columns x-1..x+1 and the Pi_k+/Pi_k- row sums, rows
+         * y-1, y (slots 0, 1); slot 2 is filled from the stage */
+        double ph[3][3], rk[3], rm[3];
         if (active) {
 #pragma unroll
             for (int slot = 0; slot < 2; slot++) {
                 const int rr = it.y - 1 + slot;
                 const int rc = clamp_row(rr, Ny);
                 const double *row = s.phi + (long long)rc * P;
-                const double pL = W ? s.phiW[rc] : row[x - 1];
-                const double pM = row[x];
-                const double pR = E ? s.phiE[rc] : row[x + 1];
-                ap[slot][0] = bgk::aplus(pL); ap[slot][1] = bgk::aplus(pM); ap[slot][2] = bgk::aplus(pR);
-                am[slot][0] = bgk::aminus(pL); am[slot][1] = bgk::aminus(pM); am[slot][2] = bgk::aminus(pR);
-                pc[slot] = pM;
+                ph[slot][0] = W ? s.phiW[rc] : row[x - 1];
+                ph[slot][1] = row[x];
+                ph[slot][2] = E ? s.phiE[rc] : row[x + 1];
                 if (rr >= 0) {
                     rk[slot] = row3(PIN + 18 * pl + (long long)rr * P, x, hasL, hasR);
                     rm[slot] = row3(PIN + 19 * pl + (long long)rr * P, x, hasL, hasR);
@@ -519,7 +535,8 @@ adj_pipe_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
                 failed = true;
                 break;
             }
-            const double *stg = reinterpret_cast<const double *>(stages + (size_t)st * ADJ_STAGE_BYTES);
+            double *stg = reinterpret_cast<double *>(stages + (size_t)st * ADJ_STAGE_BYTES);
+            bool wrote = false;
             if (active) {
                 const bool S = (y == 0), N = (y == Ny - 1);
                 const long long cc = (long long)y * P + x;
@@ -528,12 +545,9 @@ adj_pipe_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
                 {
                     const int rc = clamp_row(y + 1, Ny);
                     const double *sph = stg + 39 * ADJ_RW;
-                    const double pL = W ? s.phiW[rc] : sph[col - 1];
-                    const double pM = sph[col];
-                    const double pR = E ? s.phiE[rc] : sph[col + 1];
-                    ap[2][0] = bgk::aplus(pL); ap[2][1] = bgk::aplus(pM); ap[2][2] = bgk::aplus(pR);
-                    am[2][0] = bgk::aminus(pL); am[2][1] = bgk::aminus(pM); am[2][2] = bgk::aminus(pR);
-                    pc[2] = pM;
+                    ph[2][0] = W ? s.phiW[rc] : sph[col - 1];
+                    ph[2][1] = sph[col];
+                    ph[2][2] = E ? s.phiE[rc] : sph[col + 1];
                     if (y + 1 < Ny) {
                         rk[2] = row3(stg + 18 * ADJ_RW, col, hasL, hasR);
                         rm[2] = row3(stg + 19 * ADJ_RW, col, hasL, hasR);
@@ -543,28 +557,35 @@ adj_pipe_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
                     }
                 }
 
-                /* 1. the adjoint of S(n) at this node */
-                double lf[9], lg[9];
+                /* 1. the adjoint of S(n) at this node.  lambda_f[k] and
+                 * lambda_g[k] are the stage words at (segment k or 9+k,
+                 * column x + c_kx); each such word is read by this thread
+                 * only, so a boundary node writes its own gathered value over
+                 * it and the VJP reads every lambda from the stage. */
+                if (W || E || S || N) {
+                    wrote = true;
 #pragma unroll
-                for (int k = 0; k < 9; k++) {
-                    const int xd = x + cx_of(k), yd = y + cy_of(k);
-                    const bool xin = xd >= 0 && xd < Nx, yin = yd >= 0 && yd < Ny;
-                    if (xin && yin) {
-                        lf[k] = stg[k * ADJ_RW + col + cx_of(k)];
-                    } else {
-                        /* read by this node's own bounce-back of opp(k), except
-                         * the two frozen corners (pop 6 at (Nx,1), pop 7 at (Nx,Ny)) */
-                        const bool corner6 = (k == 8) && E && S;
-                        const bool corner7 = (k == 5) && E && N;
-                        lf[k] = (corner6 || corner7) ? 0.0 : PIN[opp_of(k) * pl + cc];
+                    for (int k = 0; k < 9; k++) {
+                        const int xd = x + cx_of(k), yd = y + cy_of(k);
+                        const bool xin = xd >= 0 && xd < Nx, yin = yd >= 0 && yd < Ny;
+                        double *wf = stg + k * ADJ_RW + col + cx_of(k);
+                        double *wg = stg + (9 + k) * ADJ_RW + col + cx_of(k);
+                        if (!(xin && yin)) {
+                            /* read by this node's own bounce-back of opp(k),
+                             * except the two frozen corners (pop 6 at (Nx,1),
+                             * pop 7 at (Nx,Ny)) */
+                            const bool corner6 = (k == 8) && E && S;
+                            const bool corner7 = (k == 5) && E && N;
+                            *wf = (corner6 || corner7) ? 0.0 : PIN[opp_of(k) * pl + cc];
+                        }
+                        double a = 0.0;
+                        if (xin) {
+                            if (yin) a += *wg;
+                            if (cy_of(k) == 1 && S) a += PIN[(9 + k) * pl + xd];
+                            if (cy_of(k) == -1 && N) a += PIN[(9 + k) * pl + (long long)(Ny - 1) * P + xd];
+                        }
+                        *wg = a;
                     }
-                    double a = 0.0;
-                    if (xin) {
-                        if (yin) a += stg[(9 + k) * ADJ_RW + col + cx_of(k)];
-                        if (cy_of(k) == 1 && S) a += PIN[(9 + k) * pl + xd];
-                        if (cy_of(k) == -1 && N) a += PIN[(9 + k) * pl + (long long)(Ny - 1) * P + xd];
-                    }
-                    lg[k] = a;
                 }
                 const double skp = rk[0] + rk[1] + rk[2] + (S ? rk[1] : 0.0) + (N ? rk[1] : 0.0);
                 const double skm = rm[0] + rm[1] + rm[2] + (S ? rm[1] : 0.0) + (N ? rm[1] : 0.0);
@@ -625,33 +646,38 @@ adj_pipe_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
                     g[6] = sg[6 * ADJ_RW + col + 1];
                     g[7] = sg[7 * ADJ_RW + col + 1];
                 }
-                const double kp = ap[1][1] + ap[1][2] + ap[2][1] + ap[1][0] + ap[0][1] + ap[2][2] + ap[2][0] +
-                                  ap[0][0] + ap[0][2];
-                const double km = am[1][1] + am[1][2] + am[2][1] + am[1][0] + am[0][1] + am[2][2] + am[2][0] +
-                                  am[0][0] + am[0][2];
+                /* selector sums in the forward kernel's order */
+                const double kp = bgk::aplus(ph[1][1]) + bgk::aplus(ph[1][2]) + bgk::aplus(ph[2][1]) +
+                                  bgk::aplus(ph[1][0]) + bgk::aplus(ph[0][1]) + bgk::aplus(ph[2][2]) +
+                                  bgk::aplus(ph[2][0]) + bgk::aplus(ph[0][0]) + bgk::aplus(ph[0][2]);
+                const double km = bgk::aminus(ph[1][1]) + bgk::aminus(ph[1][2]) + bgk::aminus(ph[2][1]) +
+                                  bgk::aminus(ph[1][0]) + bgk::aminus(ph[0][1]) + bgk::aminus(ph[2][2]) +
+                                  bgk::aminus(ph[2][0]) + bgk::aminus(ph[0][0]) + bgk::aminus(ph[0][2]);
 
                 /* 3. vector-Jacobian product -> Pi(n) */
-                double fb[9], gbv[9], kpb, kmb, p0b, omg_b;
-                node_vjp(c, s.tanh_mode, f, g, kp, km, pc[1], lf, lg, d0, skp, skm, lT, fb, gbv, kpb, kmb, p0b,
-                         omg_b);
+                const double *lam = stg + col;
+                double *po = s.pout + cc;
+                double kpb, kmb, p0b, omg_b;
+                node_vjp(c, s.tanh_mode, f, g, kp, km, ph[1][1],
+                         [&](int k) { return lam[k * ADJ_RW + cx_of(k)]; },
+                         [&](int k) { return lam[(9 + k) * ADJ_RW + cx_of(k)]; }, d0, skp, skm, lT,
+                         [&](int k, double v) { po[k * pl] = v; }, [&](int k, double v) { po[(9 + k) * pl] = v; },
+                         kpb, kmb, p0b, omg_b);
                 omg_sum += omg_b;
-#pragma unroll
-                for (int k = 0; k < 9; k++) {
-                    s.pout[k * pl + cc] = fb[k];
-                    s.pout[(9 + k) * pl + cc] = gbv[k];
-                }
                 s.pout[18 * pl + cc] = kpb;
                 s.pout[19 * pl + cc] = kmb;
                 s.pout[20 * pl + cc] = p0b;
 #pragma unroll
                 for (int k = 0; k < 3; k++) {
-                    ap[0][k] = ap[1][k]; ap[1][k] = ap[2][k];
-                    am[0][k] = am[1][k]; am[1][k] = am[2][k];
+                    ph[0][k] = ph[1][k];
+                    ph[1][k] = ph[2][k];
                 }
-                pc[0] = pc[1]; pc[1] = pc[2];
                 rk[0] = rk[1]; rk[1] = rk[2];
                 rm[0] = rm[1]; rm[1] = rm[2];
             }
+            /* generic-proxy writes into the stage are ordered before the
+             * producer's next bulk copy into it */
+            if (__any_sync(0xffffffffu, wrote)) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[st]);
             r++;

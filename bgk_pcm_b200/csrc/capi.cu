@@ -364,7 +364,7 @@ int bgk_create(const bgk_params *pp, const bgk_options *opt, bgk_ctx **out)
     if (rc) return rc;
     bgk_options o{BGK_PREC_F64, BGK_TANH_DEVICE, 0, -1, 0};
     if (opt) o = *opt;
-    if (o.precision < BGK_PREC_F64 || o.precision > BGK_PREC_F16) return fail(BGK_ERR_ARG, "bad precision %d", o.precision);
+    if (o.precision < BGK_PREC_F64 || o.precision > BGK_PREC_F32X) return fail(BGK_ERR_ARG, "bad precision %d", o.precision);
     if (o.tanh_mode != BGK_TANH_DEVICE && o.tanh_mode != BGK_TANH_PORTABLE) return fail(BGK_ERR_ARG, "bad tanh_mode");
     if (o.precision != BGK_PREC_F64 && !all_bc4(*pp))
         return fail(BGK_ERR_UNSUPPORTED, "reduced-precision forms implement the no-slip code 4 on every wall only");
@@ -398,12 +398,13 @@ int bgk_create(const bgk_params *pp, const bgk_options *opt, bgk_ctx **out)
     c->A = (size_t)c->NX2 * (size_t)c->NY2;
     c->P = (pp->Nx + 31) / 32 * 32;
     c->plane = (long long)c->P * pp->Ny;
-    c->esz = o.precision == BGK_PREC_F64 ? 8 : (o.precision == BGK_PREC_F32 ? 4 : 2);
-    /* reduced-precision forms keep phi in FP64 unless BGK_LP_PHI32=1 */
-    c->phisz = 8;
-    if (o.precision != BGK_PREC_F64) {
-        const char *v = getenv("BGK_LP_PHI32");
-        if (v && atoi(v) == 1) c->phisz = 4;
+    c->esz = o.precision == BGK_PREC_F64 ? 8 : (o.precision == BGK_PREC_F16 ? 2 : 4);
+    /* phi: FP64 in the FP64 and FP32X forms; FP32 (storage and phase-field
+     * arithmetic) in the FP32 and FP16 forms unless BGK_LP_PHI64=1 */
+    c->phisz = (o.precision == BGK_PREC_F64 || o.precision == BGK_PREC_F32X) ? 8 : 4;
+    if (o.precision == BGK_PREC_F32 || o.precision == BGK_PREC_F16) {
+        const char *v = getenv("BGK_LP_PHI64");
+        if (v && atoi(v) == 1) c->phisz = 8;
     }
     c->it = 0;
     c->cur = 0;

@@ -11,7 +11,7 @@
  * reference's own main.f90 against the C ABI (the binding a Fortran host
  * would use is bgk_pcm_b200/fortran/bgk_c.f90).
  *
- * usage: bgk_thermal [dir] [--precision f64|f32|f16] [--fma] [--tanh portable]
+ * usage: bgk_thermal [dir] [--precision f64|f32|f16|f32x] [--fma] [--tanh portable]
  *                    [--snapshot-in file] [--snapshot-out file]
  */
 #include <cmath>
@@ -283,7 +283,8 @@ int main(int argc, char **argv)
         std::string s = argv[a];
         if (s == "--precision" && a + 1 < argc) {
             std::string v = argv[++a];
-            opt.precision = v == "f32" ? BGK_PREC_F32 : (v == "f16" ? BGK_PREC_F16 : BGK_PREC_F64);
+            opt.precision = v == "f32" ? BGK_PREC_F32
+                          : (v == "f16" ? BGK_PREC_F16 : (v == "f32x" ? BGK_PREC_F32X : BGK_PREC_F64));
         } else if (s == "--fma") {
             opt.fma = 1;
         } else if (s == "--tanh" && a + 1 < argc) {

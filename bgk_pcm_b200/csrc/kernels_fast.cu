@@ -676,10 +676,9 @@ cudaError_t launch_lowp_t(bgk_ctx *c, bool moments)
 cudaError_t launch_fused_lowp(bgk_ctx *c, bool moments)
 {
     const bool p64 = c->phisz == 8;
-    if (c->opt.precision == BGK_PREC_F32) {
-        if (c->opt.fma == 2) return launch_lowp_t<float, double, double>(c, moments);   /* FP64 arithmetic */
+    if (c->opt.precision == BGK_PREC_F32X) return launch_lowp_t<float, double, double>(c, moments);
+    if (c->opt.precision == BGK_PREC_F32)
         return p64 ? launch_lowp_t<float, double, float>(c, moments) : launch_lowp_t<float, float, float>(c, moments);
-    }
     return p64 ? launch_lowp_t<__half, double, float>(c, moments) : launch_lowp_t<__half, float, float>(c, moments);
 }
 
@@ -718,7 +717,7 @@ cudaError_t launch_init_lowp(bgk_ctx *c)
 #define BGK_INIT(S, PT, sf_, sg_)                                                                        \
     init_lowp_kernel<S, PT><<<grd, blk, 0, c->stream>>>(c->c, (S *)fb, (S *)gb, (PT *)c->phibuf[0],     \
                                                         (PT *)c->phibuf[1], c->plane, c->P, sf_, sg_)
-    if (c->opt.precision == BGK_PREC_F32) {
+    if (c->opt.precision != BGK_PREC_F16) {
         if (p64) BGK_INIT(float, double, 1.f, 1.f); else BGK_INIT(float, float, 1.f, 1.f);
     } else {
         if (p64) BGK_INIT(__half, double, c->scale.sf, c->scale.sg);
@@ -793,12 +792,12 @@ static int lp_to_ref(bgk_ctx *c, int field, double *ref, int prev)
 
 int lowp_ref_to_compact(bgk_ctx *c, int field, const double *ref)
 {
-    return c->opt.precision == BGK_PREC_F32 ? bgk::lp_to_compact<float>(c, field, ref)
+    return c->opt.precision != BGK_PREC_F16 ? bgk::lp_to_compact<float>(c, field, ref)
                                             : bgk::lp_to_compact<__half>(c, field, ref);
 }
 
 int lowp_compact_to_ref(bgk_ctx *c, int field, double *ref, int prev)
 {
-    return c->opt.precision == BGK_PREC_F32 ? bgk::lp_to_ref<float>(c, field, ref, prev)
+    return c->opt.precision != BGK_PREC_F16 ? bgk::lp_to_ref<float>(c, field, ref, prev)
                                             : bgk::lp_to_ref<__half>(c, field, ref, prev);
 }

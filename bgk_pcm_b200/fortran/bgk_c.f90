@@ -8,7 +8,7 @@ module bgk_c
   implicit none
 
   integer(c_int), parameter :: BGK_OK = 0
-  integer(c_int), parameter :: BGK_PREC_F64 = 0, BGK_PREC_F32 = 1, BGK_PREC_F16 = 2
+  integer(c_int), parameter :: BGK_PREC_F64 = 0, BGK_PREC_F32 = 1, BGK_PREC_F16 = 2, BGK_PREC_F32X = 3
   integer(c_int), parameter :: BGK_TANH_DEVICE = 0, BGK_TANH_PORTABLE = 1
   integer(c_int), parameter :: BGK_FIELD_F0 = 0, BGK_FIELD_G0 = 9
   integer(c_int), parameter :: BGK_FIELD_RHO = 18, BGK_FIELD_T = 19, BGK_FIELD_U = 20, BGK_FIELD_V = 21

@@ -19,7 +19,7 @@ import numpy as np
 
 from . import capi
 
-_PREC = {"f64": capi.PREC_F64, "f32": capi.PREC_F32, "f16": capi.PREC_F16}
+_PREC = {"f64": capi.PREC_F64, "f32": capi.PREC_F32, "f16": capi.PREC_F16, "f32x": capi.PREC_F32X}
 _TANH = {"device": capi.TANH_DEVICE, "portable": capi.TANH_PORTABLE}
 
 

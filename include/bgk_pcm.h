@@ -56,6 +56,7 @@ typedef struct bgk_params {
 #define BGK_PREC_F64   0  /* plain FP64 (the reference's mykind = dp)                  */
 #define BGK_PREC_F32   1  /* FP32 deviations f_i - w_i*rho0, g_i - w_i*T0, FP32 math    */
 #define BGK_PREC_F16   2  /* FP16 deviations with a per-field scale, FP32 math          */
+#define BGK_PREC_F32X  3  /* FP32 deviations, FP64 math, phi in FP64                   */
 
 /* tanh used by the phase-field selector (STEP_7/phase_field.f90:20-21). */
 #define BGK_TANH_DEVICE   0  /* CUDA's tanh (production)                              */
