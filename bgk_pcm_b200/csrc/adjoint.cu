@@ -27,6 +27,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <vector>
 
 #include "bgk_internal.h"
@@ -83,20 +84,6 @@ __device__ __forceinline__ double poly_k(int k, double u, double v, double &du, 
     return 1.0 + 3.0 * cu + 4.5 * cu * cu - 1.5 * (u * u + v * v);
 }
 
-/* dP_k/du and dP_k/dv of the equilibrium polynomials (see eq_poly). */
-__device__ __forceinline__ void eq_poly_grad(double u, double v, double *du, double *dv)
-{
-    const double upv = u + v, umv = u - v;
-    du[0] = -3.0 * u;                     dv[0] = -3.0 * v;
-    du[1] = 3.0 + 6.0 * u;                dv[1] = -3.0 * v;
-    du[2] = -3.0 * u;                     dv[2] = 3.0 + 6.0 * v;
-    du[3] = -3.0 + 6.0 * u;               dv[3] = -3.0 * v;
-    du[4] = -3.0 * u;                     dv[4] = -3.0 + 6.0 * v;
-    du[5] = 3.0 + 9.0 * upv - 3.0 * u;    dv[5] = 3.0 + 9.0 * upv - 3.0 * v;
-    du[6] = -3.0 + 9.0 * umv - 3.0 * u;   dv[6] = 3.0 - 9.0 * umv - 3.0 * v;
-    du[7] = -3.0 + 9.0 * upv - 3.0 * u;   dv[7] = -3.0 + 9.0 * upv - 3.0 * v;
-    du[8] = 3.0 + 9.0 * umv - 3.0 * u;    dv[8] = -3.0 - 9.0 * umv - 3.0 * v;
-}
 
 /* Vector-Jacobian product of one node update (smooth form).
  * in : pulled f, g; selector sums kp, km; phi_prec p0; output adjoints
@@ -775,9 +762,6 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
     for (int p = 0; p < spec->nprobes; p++)
         if (spec->probe_i[p] < 1 || spec->probe_i[p] > c->Nx || spec->probe_j[p] < 1 || spec->probe_j[p] > c->Ny)
             return bgk_internal_fail(BGK_ERR_ARG, "probe outside 1..Nx x 1..Ny");
-    int K = spec->checkpoint_every;
-    if (K <= 0) K = (int)std::ceil(std::sqrt((double)N));
-    if (K > N) K = N;
     int rc = bgk_internal_prepare_fused(c);
     if (rc) return rc;
 
@@ -791,7 +775,36 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
     const long long tc_pad = ((long long)Ny + 31) / 32 * 32;
     const size_t state_guard = 256;     /* elements on each side */
     const size_t state_elems = (size_t)(19 * pl + tc_pad) + 2 * state_guard;
+    const size_t state_bytes = state_elems * sizeof(double);
+
+    /* Checkpoint schedule.  K > 0: snapshots every K steps, each K-step
+     * segment recomputed into a buffer of K + 1 states and reversed (the
+     * sqrt(N) scheme; K = ceil(sqrt(N)) when checkpoint_every is 0).  When
+     * that does not fit in free device memory, or when checkpoint_every < 0,
+     * a binomial schedule (Griewank's revolve, written as a recursion) with
+     * a fixed number of state slots: -checkpoint_every of them, or as many
+     * as fit.  Both give the same gradient bit for bit. */
+    int K = spec->checkpoint_every > 0 ? spec->checkpoint_every : (int)std::ceil(std::sqrt((double)N));
+    if (K > N) K = N;
     const int nsnap = (N + K - 1) / K;    /* snapshots of S(0), S(K), ...    */
+    const size_t fixed_bytes = 2 * ((size_t)NPI * pl + 2 * state_guard) * sizeof(double) + 8 * (size_t)Ny * 8 +
+                               (64u << 20);
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return bgk_internal_fail(BGK_ERR_CUDA, "cudaMemGetInfo failed");
+    }
+    const size_t margin = (size_t)1 << 30;
+    const size_t avail = free_b > fixed_bytes + margin ? free_b - fixed_bytes - margin : 0;
+    bool binomial = spec->checkpoint_every < 0 || (size_t)(nsnap + K + 1) * state_bytes > avail;
+    int nslots = 0;                        /* binomial: state slots incl. S(0) */
+    if (binomial) {
+        nslots = spec->checkpoint_every < 0 ? -spec->checkpoint_every : (int)(avail / state_bytes) - 3;
+        if (nslots > N) nslots = N;
+        if (nslots < 1 || (size_t)(nslots + 3) * state_bytes > avail)
+            return bgk_internal_fail(BGK_ERR_OOM, "not enough device memory for the adjoint's checkpoints");
+    }
+
     std::vector<void *> allocs;
     auto dmalloc = [&](size_t bytes) -> double * {
         void *p = nullptr;
@@ -800,10 +813,14 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
         return (double *)p;
     };
     auto cleanup = [&]() { for (void *p : allocs) cudaFree(p); };
-    double *snaps_raw = dmalloc((size_t)nsnap * state_elems * sizeof(double));
-    double *seg_raw = dmalloc((size_t)(K + 1) * state_elems * sizeof(double));
-    double *snaps = snaps_raw ? snaps_raw + state_guard : nullptr;   /* state i at snaps + i*state_elems */
-    double *seg = seg_raw ? seg_raw + state_guard : nullptr;
+    /* sqrt(N): nsnap snapshots + K+1 segment states; binomial: nslots slots
+     * + 3 work states.  State i of a block at base + i * state_elems. */
+    const size_t nstates_a = binomial ? (size_t)nslots : (size_t)nsnap;
+    const size_t nstates_b = binomial ? 3 : (size_t)(K + 1);
+    double *blk_a_raw = dmalloc(nstates_a * state_bytes);
+    double *blk_b_raw = dmalloc(nstates_b * state_bytes);
+    double *snaps = blk_a_raw ? blk_a_raw + state_guard : nullptr;
+    double *seg = blk_b_raw ? blk_b_raw + state_guard : nullptr;
     /* partial planes Pi, guarded like the states (the pipelined reverse step
      * copies row segments of them) */
     double *pi_raw[2] = {dmalloc(((size_t)NPI * pl + 2 * state_guard) * sizeof(double)),
@@ -842,6 +859,29 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
             return e;
         return cudaMemcpyAsync(dst + 19 * pl, c->tcol[buf], Ny * sizeof(double), cudaMemcpyDeviceToDevice, st);
     };
+    /* one fused forward step between two stored states */
+    auto fwd = [&](const double *a, double *b) -> cudaError_t {
+        return bgk::launch_fused_f64_ptrs(c, a, a + 9 * pl, a + 18 * pl, a + 19 * pl, b, b + 9 * pl, b + 18 * pl,
+                                          b + 19 * pl);
+    };
+    /* one reverse step: forward step n, from S(n-1) */
+    int pin = 0;
+    auto rstep = [&](const double *S0) -> cudaError_t {
+        AdjPtrs a{};
+        a.f = S0; a.g = S0 + 9 * pl; a.phi = S0 + 18 * pl; a.tcol = S0 + 19 * pl;
+        a.pin = pi[pin]; a.pout = pi[pin ^ 1];
+        a.gW = c->gW; a.pE = c->pE; a.phiW = c->phiW; a.phiE = c->phiE; a.corner = c->corner;
+        a.omg_acc = omg_acc;
+        a.dgW = dgW; a.gtin = gtin;
+        a.plane = pl; a.P = c->P;
+        a.tanh_mode = c->opt.tanh_mode;
+        if (use_pipe)
+            adj_pipe_kernel<<<pgrid, PIPE_THREADS, ADJ_SMEM, st>>>(a, c->c, psch, c->errflag);
+        else
+            adj_step_kernel<<<grd, blk, 0, st>>>(a, c->c);
+        pin ^= 1;
+        return cudaGetLastError();
+    };
 
     if (use_pipe) {
         static std::atomic<unsigned long long> done{0};
@@ -853,13 +893,19 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
     adj_dgw_kernel<<<(Ny + 127) / 128, 128, 0, st>>>(c->c, c->mu, c->mv, dgW);
     ACK(cudaGetLastError());
 
-    /* forward pass on the context, snapshots every K steps */
+    /* forward pass on the context (snapshots every K steps in the sqrt(N)
+     * scheme; S(0) only in the binomial one) */
     ACK(copy_state_in(snaps, c->cur));
-    for (int n0 = 0; n0 < N; n0 += K) {
-        const int len = (n0 + K < N) ? K : N - n0;
-        rc = bgk_step(c, len);
+    if (binomial) {
+        rc = bgk_step(c, N);
         if (rc) { cleanup(); return rc; }
-        if (n0 + len < N) ACK(copy_state_in(snaps + (size_t)((n0 + len) / K) * state_elems, c->cur));
+    } else {
+        for (int n0 = 0; n0 < N; n0 += K) {
+            const int len = (n0 + K < N) ? K : N - n0;
+            rc = bgk_step(c, len);
+            if (rc) { cleanup(); return rc; }
+            if (n0 + len < N) ACK(copy_state_in(snaps + (size_t)((n0 + len) / K) * state_elems, c->cur));
+        }
     }
     /* loss and seed */
     ACK(cudaMemsetAsync(pi[0], 0, (size_t)NPI * pl * sizeof(double), st));
@@ -869,37 +915,79 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
                                       pi[0] + 20 * pl, scal);
     ACK(cudaGetLastError());
 
-    /* reverse sweep, one segment at a time */
-    int pin = 0;
-    for (int sgi = nsnap - 1; sgi >= 0; sgi--) {
-        const int n0 = sgi * K;
-        const int n1 = (n0 + K < N) ? n0 + K : N;
-        /* states S(n0) .. S(n1-1) into seg[0 .. n1-n0-1] */
-        ACK(cudaMemcpyAsync(seg, snaps + (size_t)sgi * state_elems, (state_elems - 2 * state_guard) * sizeof(double),
-                            cudaMemcpyDeviceToDevice, st));
-        for (int n = n0 + 1; n < n1; n++) {
-            double *a = seg + (size_t)(n - 1 - n0) * state_elems;
-            double *b = seg + (size_t)(n - n0) * state_elems;
-            ACK(bgk::launch_fused_f64_ptrs(c, a, a + 9 * pl, a + 18 * pl, a + 19 * pl, b, b + 9 * pl, b + 18 * pl,
-                                           b + 19 * pl));
+    if (!binomial) {
+        /* reverse sweep, one segment at a time */
+        for (int sgi = nsnap - 1; sgi >= 0; sgi--) {
+            const int n0 = sgi * K;
+            const int n1 = (n0 + K < N) ? n0 + K : N;
+            /* states S(n0) .. S(n1-1) into seg[0 .. n1-n0-1] */
+            ACK(cudaMemcpyAsync(seg, snaps + (size_t)sgi * state_elems,
+                                (state_elems - 2 * state_guard) * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            for (int n = n0 + 1; n < n1; n++)
+                ACK(fwd(seg + (size_t)(n - 1 - n0) * state_elems, seg + (size_t)(n - n0) * state_elems));
+            for (int n = n1; n > n0; n--) ACK(rstep(seg + (size_t)(n - 1 - n0) * state_elems));
         }
-        for (int n = n1; n > n0; n--) {
-            const double *S0 = seg + (size_t)(n - 1 - n0) * state_elems;
-            AdjPtrs a{};
-            a.f = S0; a.g = S0 + 9 * pl; a.phi = S0 + 18 * pl; a.tcol = S0 + 19 * pl;
-            a.pin = pi[pin]; a.pout = pi[pin ^ 1];
-            a.gW = c->gW; a.pE = c->pE; a.phiW = c->phiW; a.phiE = c->phiE; a.corner = c->corner;
-            a.omg_acc = omg_acc;
-            a.dgW = dgW; a.gtin = gtin;
-            a.plane = pl; a.P = c->P;
-            a.tanh_mode = c->opt.tanh_mode;
-            if (use_pipe)
-                adj_pipe_kernel<<<pgrid, PIPE_THREADS, ADJ_SMEM, st>>>(a, c->c, psch, c->errflag);
-            else
-                adj_step_kernel<<<grd, blk, 0, st>>>(a, c->c);
-            ACK(cudaGetLastError());
-            pin ^= 1;
-        }
+    } else {
+        double *work[3] = {seg, seg + state_elems, seg + 2 * state_elems};
+        auto slot = [&](int i) { return snaps + (size_t)i * state_elems; };
+        /* S(a + steps) from S(a) in src into dst (dst is a slot or work[2]) */
+        auto advance = [&](const double *src, int steps, double *dst) -> cudaError_t {
+            const double *cur = src;
+            int w = 0;
+            for (int i = 1; i <= steps; i++) {
+                double *next = (i == steps) ? dst : work[w];
+                cudaError_t e = fwd(cur, next);
+                if (e != cudaSuccess) return e;
+                cur = next;
+                w ^= 1;
+            }
+            return cudaSuccess;
+        };
+        /* C(cp + r, cp): steps reversible with cp checkpoints and r repetitions */
+        auto beta = [](int cp, int r) {
+            double v = 1.0;
+            for (int i = 1; i <= cp; i++) v = v * (double)(r + i) / (double)i;
+            return v;
+        };
+        /* reverse forward steps b, b-1, ..., a+1; S(a) is in slot ia; slots
+         * ia+1 .. nslots-1 are free */
+        std::function<cudaError_t(int, int, int)> rev = [&](int a, int b, int ia) -> cudaError_t {
+            const int n = b - a;
+            const int nfree = nslots - 1 - ia;
+            cudaError_t e;
+            if (n == 1) return rstep(slot(ia));
+            if (nfree == 0) {
+                for (int k = b; k > a; k--) {
+                    if (k - 1 == a) {
+                        e = rstep(slot(ia));
+                    } else {
+                        if ((e = advance(slot(ia), k - 1 - a, work[2])) != cudaSuccess) return e;
+                        e = rstep(work[2]);
+                    }
+                    if (e != cudaSuccess) return e;
+                }
+                return cudaSuccess;
+            }
+            /* fewest repetitions r with C(cp + r, cp) >= n; the first
+             * checkpoint goes l steps ahead, l in [n - C(cp - 1 + r, cp - 1),
+             * C(cp + r - 1, cp)] (right part reversible with one checkpoint
+             * less, left part with one repetition less); the middle of that
+             * range is within ~1 % of the fewest forward steps */
+            const int cp = nfree + 1;
+            int r = 0;
+            while (beta(cp, r) < (double)n) r++;
+            const double rmax = beta(cp - 1, r), lmax = beta(cp, r - 1);
+            const int lo = rmax >= (double)(n - 1) ? 1 : n - (int)rmax;
+            const int hi = lmax >= (double)(n - 1) ? n - 1 : (int)lmax;
+            int l = (lo + hi) / 2;
+            if (l < 1) l = 1;
+            if (l > n - 1) l = n - 1;
+            const int m = a + l;
+            if ((e = advance(slot(ia), l, slot(ia + 1))) != cudaSuccess) return e;
+            if ((e = rev(m, b, ia + 1)) != cudaSuccess) return e;
+            return rev(a, m, ia);
+        };
+        ACK(rev(0, N, 0));
     }
     adj_tin_kernel<<<1, 1024, 0, st>>>(pi[pin], pl, c->P, Ny, dgW, gtin);
     ACK(cudaGetLastError());

@@ -183,7 +183,11 @@ int bgk_get_stream(bgk_ctx *ctx, void **stream);
  * nsteps fused steps from the current state. */
 typedef struct bgk_adjoint_spec {
     int nsteps;                /* forward steps from the current state           */
-    int checkpoint_every;      /* snapshot interval K (<= 0: ceil(sqrt(nsteps)))  */
+    int checkpoint_every;      /* K > 0: snapshot every K steps; 0: K =
+                                * ceil(sqrt(nsteps)), or the binomial schedule
+                                * when those snapshots do not fit in free
+                                * device memory; < 0: binomial schedule with
+                                * -checkpoint_every state slots               */
     int nprobes;
     const int *probe_i;        /* reference indices, 1..Nx                       */
     const int *probe_j;        /* 1..Ny                                          */
@@ -195,7 +199,9 @@ typedef struct bgk_adjoint_spec {
  * per row by bgk_set_tin) and to the thermal relaxation time tau_g
  * (STEP_7/setup.f90:103), by a hand-written reverse of the fused step run
  * backward in time with checkpoint-and-recompute: snapshots every K steps,
- * each K-step segment recomputed forward before it is reversed.  No
+ * each K-step segment recomputed forward before it is reversed, or, when
+ * memory is short, a binomial (revolve) schedule over a fixed number of
+ * state slots that recomputes each step a few times instead.  No
  * reference counterpart (the reference has no derivatives).  Requires an FP64
  * context created with opt.smooth = 1 (the differentiable form).  The
  * context is left at the final state, exactly as bgk_step(ctx, nsteps)

@@ -62,6 +62,21 @@ def test_adjoint_requires_smooth(lib):
         s.adjoint(3, [2], [2], [0.0])
 
 
+@pytest.mark.parametrize("slots", [1, 2, 3, 7])
+def test_adjoint_binomial_schedule_matches_sqrt_schedule(lib, slots):
+    """checkpoint_every < 0 selects the memory-bounded binomial schedule with
+    that many state slots (the one a grid too large for sqrt(N) snapshots
+    falls back to); every reverse step sees the same forward state, so the
+    gradient is identical bit for bit."""
+    from bgk_pcm_b200 import gradcheck as gc
+    p, tin, tin_t, pi, pj = gc.setup(Nx=40, Ny=33, steps=23, nprobes=10, **SENSITIVE)
+    target = gc.forward_phi(p, tin_t, 23, pi, pj)
+    a = gc.adjoint(p, tin, 23, pi, pj, target, checkpoint_every=5)
+    b = gc.adjoint(p, tin, 23, pi, pj, target, checkpoint_every=-slots)
+    assert a[0] == b[0] and a[2] == b[2]
+    np.testing.assert_array_equal(a[1], b[1])
+
+
 @pytest.mark.slow
 def test_adjoint_config4_fd_16_directions(lib):
     """512x512, Ra 1e5, 2000 steps, 64 probes, checkpoints every 45 steps:
