@@ -21,6 +21,7 @@ constexpr long long PIPE_WAIT_LIMIT = 1LL << 24;   /* x ~64 ns sleeps: ~1 s */
 
 struct PipeSched {
     int nbands, H, nstrips, ntiles;
+    int bx;                 /* band (tile) width in columns */
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -89,7 +90,7 @@ struct PipeIter {
     {
         if (t >= sch.ntiles) return false;
         const int band = t % sch.nbands, strip = t / sch.nbands;
-        x0 = band * PIPE_BX;
+        x0 = band * sch.bx;
         y = strip * sch.H;
         y1 = min(y + sch.H, Ny);
         return true;
@@ -109,6 +110,7 @@ struct PipeIter {
 inline PipeSched pipe_sched(const bgk_ctx *c, int ctas_per_sm, int base_H, int *grid)
 {
     PipeSched sch;
+    sch.bx = PIPE_BX;
     sch.nbands = (c->Nx + PIPE_BX - 1) / PIPE_BX;
     const long long slots = (long long)c->nsm * ctas_per_sm;
     int H = base_H;
