@@ -528,7 +528,7 @@ adj_pipe_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
         do {
             const int y = it.y;
             const int st = (int)(r % ADJ_D);
-            if (!mbar_wait(&full[st], (uint32_t)((r / ADJ_D) & 1))) {
+            if (!__all_sync(0xffffffffu, mbar_wait(&full[st], (uint32_t)((r / ADJ_D) & 1)))) {
                 atomicExch(errflag, 13);
                 failed = true;
                 break;
@@ -705,10 +705,11 @@ adj_pipe_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
  * row).  Eight consumer warps + one producer warp per CTA, two CTAs per SM.
  * Same stage layout and producer as adj_pipe_kernel.
  * ---------------------------------------------------------------------- */
-/* exchange slots: written before the first pair barrier of a row ... */
-enum { XS_RHO = 0, XS_MX, XS_MY, XS_KP, XS_KM, XS_P0, XS_T,
-       /* ... and before the second */
-       XS_UFB_F, XS_VFB_F, XS_RHOB_F, XS_UFB_G, XS_VFB_G, XS_TFB_G, XS_PHNB, XS_HT, AP_XS };
+/* exchange slots.  Written before the first pair barrier of a row and read
+ * after both barriers (so kept in two copies, by row parity) ... */
+enum { XS_RHO = 0, XS_MX, XS_MY, XS_KP, XS_KM, XS_P0, XS_T, XS_NFWD,
+       /* ... and written before the second barrier, read after it */
+       XS_UFB_F = 2 * XS_NFWD, XS_VFB_F, XS_RHOB_F, XS_UFB_G, XS_VFB_G, XS_TFB_G, XS_PHNB, XS_HT, AP_XS };
 
 /* Geometry of the warp-pair kernel with PAIRS pairs (band of 32*PAIRS
  * columns) and CTAS CTAs per SM. */
@@ -768,8 +769,18 @@ adj_pair_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
     double *xbase = reinterpret_cast<double *>(smem + ADJ_HEADER + (size_t)ADJ_D * G::STAGE_BYTES);
     double *xch = xbase + (size_t)pair * AP_XS * 32;
     volatile int *okx = reinterpret_cast<volatile int *>(xbase + (size_t)PAIRS * AP_XS * 32) + 2 * pair;
-    auto X = [&](int slot) -> double & { return xch[slot * 32 + lane]; };
-    auto pair_sync = [&]() { asm volatile("bar.sync %0, 64;" ::"r"(1 + pair) : "memory"); };
+    int par = 0;      /* row parity: which copy of the first-barrier slots */
+    auto X = [&](int slot) -> double & {
+        return xch[(slot < XS_NFWD ? slot + par * XS_NFWD : slot) * 32 + lane];
+    };
+    /* named barrier of the two warps of a pair (64 threads).  Both warps
+     * reach each one at the same point of every row, with all lanes (the
+     * code before it is warp-uniform at the call); __syncwarp() first
+     * reconverges the lanes, and the non-aligned form counts threads. */
+    auto pair_sync = [&]() {
+        __syncwarp();
+        asm volatile("barrier.sync %0, 64;" ::"r"(1 + pair) : "memory");
+    };
 
     const long long pl = s.plane;
     const int P = s.P;
@@ -811,7 +822,9 @@ adj_pair_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
         do {
             const int y = it.y;
             const int st = (int)(r % ADJ_D);
-            const bool got = mbar_wait(&full[st], (uint32_t)((r / ADJ_D) & 1));
+            par = (int)(r & 1);
+            /* warp-uniform: a lane whose bounded wait gave up fails the whole warp */
+            const bool got = __all_sync(0xffffffffu, mbar_wait(&full[st], (uint32_t)((r / ADJ_D) & 1)));
             double *stg = reinterpret_cast<double *>(stages + (size_t)st * G::STAGE_BYTES);
             const bool S = (y == 0), N = (y == Ny - 1);
             const long long cc = (long long)y * P + x;
@@ -938,6 +951,7 @@ adj_pair_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
                 if (flow && lane == 0) atomicExch(errflag, 13);
                 failed = true;
             }
+            double axx = 0.0, ayy = 0.0, axy = 0.0;        /* pxxb.. (flow) or txxb.. (thermal) */
             if (!failed && active) {
                 /* ---- forward chain (both warps) ---- */
                 const double rho = X(XS_RHO), mx = X(XS_MX), my = X(XS_MY);
@@ -959,7 +973,6 @@ adj_pair_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
                 const double *lam = stg + col;
 
                 /* ---- own half of the collision VJP, second exchange ---- */
-                double axx = 0.0, ayy = 0.0, axy = 0.0;    /* pxxb.. (flow) or txxb.. (thermal) */
                 double ub_part = 0.0, vb_part = 0.0, sb_part = 0.0;
                 if (flow) {
                     const double cf = 1.0 - c.omega_f;
@@ -1020,7 +1033,27 @@ adj_pair_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
                     X(XS_PHNB) = d0 + 0.5 * (1.0 + phn) * skp - 0.5 * (1.0 - phn) * skm;
                     X(XS_HT) = hT;
                 }
-                pair_sync();
+            }
+            /* the second barrier is taken by every lane of both warps (the
+             * same barrier instruction for the whole warp) */
+            if (!failed) pair_sync();
+            if (!failed && active) {
+                /* the forward chain again, from the exchanged scalars */
+                const double rho = X(XS_RHO), mx = X(XS_MX), my = X(XS_MY);
+                const double kp = X(XS_KP), km = X(XS_KM), p0 = X(XS_P0), T = X(XS_T);
+                const double irho = 1.0 / rho;
+                const double u = irho * mx, v = irho * my;
+                const double th = tanh_sel(((T - c.T_crit) - c.T_act) * s.inv_T_width, s.tanh_mode);
+                const double rp = 0.5 * (1.0 + th), rm = 0.5 * (1.0 - th);
+                const double KP = (kp / 8.0) * rp, KM = (km / 8.0) * rm;
+                const double phn = p0 + (c.f_plus * KP * (1.0 - p0) - c.f_minus * KM * (1.0 + p0));
+                const double Tf = T - c.dts * (phn - p0) / 2.0;
+                const double gb = c.grav * c.beta;
+                const double onep = 1.0 + phn / 2.0;
+                const double omp = 1.0 - phn;
+                const double FX = -(u * omp * 0.5);
+                const double FY = rho * gb * Tf * onep - v * omp * 0.5;
+                const double iorho = 1.0 / (c.omega_f * rho);
                 /* ---- scalar reverse tail (both warps) ---- */
                 const double ufb = X(XS_UFB_F) + X(XS_UFB_G), vfb = X(XS_VFB_F) + X(XS_VFB_G);
                 double rhob = X(XS_RHOB_F), Tfb = X(XS_TFB_G);
@@ -1063,8 +1096,6 @@ adj_pair_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
                     }
                     po[20 * pl] = 0.5 * c.dts * Tfb + PHb * (1.0 - c.f_plus * KP - c.f_minus * KM);
                 }
-            } else if (!failed) {
-                pair_sync();       /* inactive columns take the second barrier too */
             }
             if (active) {
                 if (flow) {

@@ -143,7 +143,7 @@ fused_pipe_f64_kernel(StepPtrs<double> s, Consts c, const double *__restrict__ c
         do {
             const int y = it.y;
             const int st = (int)(r % D);
-            if (!mbar_wait(&full[st], (uint32_t)((r / D) & 1))) {
+            if (!__all_sync(0xffffffffu, mbar_wait(&full[st], (uint32_t)((r / D) & 1)))) {
                 atomicExch(errflag, 3);
                 failed = true;
                 break;

@@ -438,7 +438,7 @@ fused_pipe_lp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, PipeSched sch, int *errfla
         do {
             const int y = it.y;
             const int st = (int)(r % D);
-            if (!mbar_wait(&full[st], (uint32_t)((r / D) & 1))) {
+            if (!__all_sync(0xffffffffu, mbar_wait(&full[st], (uint32_t)((r / D) & 1)))) {
                 atomicExch(errflag, 3);
                 failed = true;
                 break;
