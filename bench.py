@@ -197,25 +197,17 @@ def e2e_run(params, precision, steps, device, torch):
 def adjoint_cost(torch, repeats=3):
     """Cost of one adjoint gradient against one forward solve on the
     differentiation workload (512^2, Ra 1e5, 2000 steps, 64 probes,
-    checkpoints every 45 steps).  Wall clock around synchronised calls, so
-    the adjoint's workspace allocation is included; best of `repeats`."""
-    from bgk_pcm_b200 import Solver, gradcheck as gc
+    checkpoints every 45 steps).  Both timed on an existing context (wall
+    clock around synchronised calls, best of `repeats`); the adjoint's
+    workspace stays in the context after a first, untimed call."""
+    from bgk_pcm_b200 import gradcheck as gc
     p, tin, tin_t, pi, pj = gc.setup()
     steps, K = p["iter"], 45
     target = gc.forward_phi(p, tin_t, steps, pi, pj)
-    fw, ad = [], []
-    for _ in range(repeats):
-        s = Solver(p, smooth=True)
-        s.initialization(); s.set_tin(tin); s.sync()
-        t0 = time.perf_counter(); s.step(steps); s.sync(); fw.append(time.perf_counter() - t0)
-        s.close()
-        s = Solver(p, smooth=True)
-        s.initialization(); s.set_tin(tin); s.sync()
-        t0 = time.perf_counter(); loss, _, _ = s.adjoint(steps, pi, pj, target, K); ad.append(time.perf_counter() - t0)
-        s.close()
+    ratio, tf, ta = gc.cost_ratio(p, tin, steps, pi, pj, target, K, repeats)
     return {"workload": "cavity512_ra1e5_adjoint", "steps": steps, "checkpoint_every": K,
-            "forward_ms": min(fw) * 1e3, "adjoint_ms": min(ad) * 1e3, "ratio": min(ad) / min(fw),
-            "loss": loss, "timing": "wall clock, synchronised, best of %d" % repeats}
+            "forward_ms": tf * 1e3, "adjoint_ms": ta * 1e3, "ratio": ratio,
+            "timing": "wall clock, synchronised, best of %d, on an existing context" % repeats}
 
 
 def run_reference(args, params, wl):

@@ -688,441 +688,6 @@ adj_pipe_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
     if (lane == 0) s.omg_acc[blockIdx.x * PIPE_CWARPS + warp] += omg_sum;
 }
 
-/* ------------------------------------------------------------------------
- * The reverse step with the node VJP split over a pair of warps (default).
- * The per-node VJP holds ~250 live registers' worth of state, so a CTA of
- * four consumer warps fits twice on an SM and each SM sub-partition has two
- * warps to switch between: latency-bound.  Here each 32-column slice of a
- * tile is handled by two warps of the same CTA:
- *   flow warp:    phi window, pulled f, lambda_f, the f-collision VJP, the
- *                 f-population adjoints, k+/k- partials;
- *   thermal warp: Pi_k+/Pi_k- window, pulled g, lambda_g, the g-collision
- *                 VJP and d/d omega_g, the g-population adjoints, phi_prec
- *                 partial, the east T column and the west Tin terms.
- * Both recompute the scalar forward chain (moments, phase field, forces)
- * and the scalar reverse tail; they exchange a few scalars per node through
- * shared memory, synchronised by a named barrier per warp pair (two per
- * row).  Eight consumer warps + one producer warp per CTA, two CTAs per SM.
- * Same stage layout and producer as adj_pipe_kernel.
- * ---------------------------------------------------------------------- */
-/* exchange slots.  Written before the first pair barrier of a row and read
- * after both barriers (so kept in two copies, by row parity) ... */
-enum { XS_RHO = 0, XS_MX, XS_MY, XS_KP, XS_KM, XS_P0, XS_T, XS_NFWD,
-       /* ... and written before the second barrier, read after it */
-       XS_UFB_F = 2 * XS_NFWD, XS_VFB_F, XS_RHOB_F, XS_UFB_G, XS_VFB_G, XS_TFB_G, XS_PHNB, XS_HT, AP_XS };
-
-/* Geometry of the warp-pair kernel with PAIRS pairs (band of 32*PAIRS
- * columns) and CTAS CTAs per SM. */
-template <int PAIRS>
-struct PairGeom {
-    static constexpr int BX = 32 * PAIRS;
-    static constexpr int CWARPS = 2 * PAIRS;
-    static constexpr int THREADS = 32 * CWARPS + 32;
-    static constexpr int RW = BX + 2 * ADJ_AL;
-    static constexpr int STAGE_BYTES = ADJ_NSEG * RW * (int)sizeof(double);
-    static constexpr size_t XBYTES = (size_t)PAIRS * AP_XS * 32 * sizeof(double) + 16 * PAIRS;
-    static constexpr size_t SMEM = (size_t)ADJ_HEADER + (size_t)ADJ_D * STAGE_BYTES + XBYTES;
-};
-
-template <int PAIRS, int CTAS>
-__global__ void __launch_bounds__(PairGeom<PAIRS>::THREADS, CTAS)
-adj_pair_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
-{
-    using G = PairGeom<PAIRS>;
-    constexpr int RW = G::RW;
-    extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem);
-    uint64_t *empty = full + ADJ_D;
-    unsigned char *stages = smem + ADJ_HEADER;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int Nx = c.Nx, Ny = c.Ny;
-    if (tid == 0) {
-        for (int d = 0; d < ADJ_D; d++) {
-            mbar_init(&full[d], 1);
-            mbar_init(&empty[d], G::CWARPS);
-        }
-        mbar_fence_init();
-    }
-    __syncthreads();
-    if (warp == G::CWARPS) {
-        if (lane != 0) return;
-        PipeIter it;
-        long long r = 0;
-        bool ok = it.start(sch, Ny);
-        while (ok) {
-            const int st = (int)(r % ADJ_D);
-            if (r >= ADJ_D && !mbar_wait(&empty[st], (uint32_t)(((r / ADJ_D) - 1) & 1))) {
-                atomicExch(errflag, 11);
-                break;
-            }
-            adj_issue_t<RW>(s, Ny, it.x0, it.y, stages + (size_t)st * G::STAGE_BYTES, &full[st]);
-            r++;
-            ok = it.next();
-        }
-        for (long long q = (r > ADJ_D ? r - ADJ_D : 0); q < r; q++)
-            if (!mbar_wait(&full[q % ADJ_D], (uint32_t)((q / ADJ_D) & 1))) atomicExch(errflag, 12);
-        return;
-    }
-
-    const int pair = warp % PAIRS;
-    const bool flow = warp < PAIRS;             /* else thermal */
-    double *xbase = reinterpret_cast<double *>(smem + ADJ_HEADER + (size_t)ADJ_D * G::STAGE_BYTES);
-    double *xch = xbase + (size_t)pair * AP_XS * 32;
-    volatile int *okx = reinterpret_cast<volatile int *>(xbase + (size_t)PAIRS * AP_XS * 32) + 2 * pair;
-    int par = 0;      /* row parity: which copy of the first-barrier slots */
-    auto X = [&](int slot) -> double & {
-        return xch[(slot < XS_NFWD ? slot + par * XS_NFWD : slot) * 32 + lane];
-    };
-    /* named barrier of the two warps of a pair (64 threads).  Both warps
-     * reach each one at the same point of every row, with all lanes (the
-     * code before it is warp-uniform at the call); __syncwarp() first
-     * reconverges the lanes, and the non-aligned form counts threads. */
-    auto pair_sync = [&]() {
-        __syncwarp();
-        asm volatile("barrier.sync %0, 64;" ::"r"(1 + pair) : "memory");
-    };
-
-    const long long pl = s.plane;
-    const int P = s.P;
-    const double *__restrict__ PIN = s.pin;
-    const double m = c.m_cs2, q = c.q_cs2;
-    double omg_sum = 0.0;
-    PipeIter it;
-    long long r = 0;
-    bool ok = it.start(sch, Ny);
-    bool failed = false;
-    while (ok && !failed) {
-        const int x = it.x0 + pair * 32 + lane;
-        const bool active = x < Nx;
-        const bool W = (x == 0), E = (x == Nx - 1);
-        const bool hasL = x > 0, hasR = x + 1 < Nx;
-        /* window rows y-1, y: phi (flow warp: wa) or the Pi_k+ / Pi_k- row
-         * sums (thermal warp: wk, wm); row y+1 comes from the stage */
-        double wa[3][3], wk[3], wm[3];
-        if (active) {
-#pragma unroll
-            for (int slot = 0; slot < 2; slot++) {
-                const int rr = it.y - 1 + slot;
-                const int rc = clamp_row(rr, Ny);
-                if (flow) {
-                    const double *row = s.phi + (long long)rc * P;
-                    wa[slot][0] = W ? s.phiW[rc] : row[x - 1];
-                    wa[slot][1] = row[x];
-                    wa[slot][2] = E ? s.phiE[rc] : row[x + 1];
-                } else if (rr >= 0) {
-                    wk[slot] = row3(PIN + 18 * pl + (long long)rr * P, x, hasL, hasR);
-                    wm[slot] = row3(PIN + 19 * pl + (long long)rr * P, x, hasL, hasR);
-                } else {
-                    wk[slot] = 0.0;
-                    wm[slot] = 0.0;
-                }
-            }
-        }
-        const int tile = it.t;
-        do {
-            const int y = it.y;
-            const int st = (int)(r % ADJ_D);
-            par = (int)(r & 1);
-            /* warp-uniform: a lane whose bounded wait gave up fails the whole warp */
-            const bool got = __all_sync(0xffffffffu, mbar_wait(&full[st], (uint32_t)((r / ADJ_D) & 1)));
-            double *stg = reinterpret_cast<double *>(stages + (size_t)st * G::STAGE_BYTES);
-            const bool S = (y == 0), N = (y == Ny - 1);
-            const long long cc = (long long)y * P + x;
-            const int col = pair * 32 + lane + ADJ_AL;
-            double *sg = stg + 30 * RW;      /* pulled g: segment k, column col - c_kx */
-            bool wrote = false;
-            double skp = 0.0, skm = 0.0, d0 = 0.0, hT = 0.0;
-            /* ---- phase 1: own inputs, first exchange ---- */
-            if (got && active) {
-                if (flow) {
-                    const int rc = clamp_row(y + 1, Ny);
-                    const double *sph = stg + 39 * RW;
-                    wa[2][0] = W ? s.phiW[rc] : sph[col - 1];
-                    wa[2][1] = sph[col];
-                    wa[2][2] = E ? s.phiE[rc] : sph[col + 1];
-                    const double *sp = stg + 21 * RW;
-                    const double *F = s.f;
-                    double f[9];
-                    f[0] = sp[0 * RW + col];
-                    f[1] = W ? sp[3 * RW + col] : sp[1 * RW + col - 1];
-                    f[2] = sp[2 * RW + col];
-                    f[3] = E ? sp[1 * RW + col] : sp[3 * RW + col + 1];
-                    f[4] = sp[4 * RW + col];
-                    f[5] = sp[5 * RW + col - 1];
-                    f[6] = sp[6 * RW + col + 1];
-                    f[7] = sp[7 * RW + col + 1];
-                    f[8] = sp[8 * RW + col - 1];
-                    if (W || E || S || N) {
-                        if (S) f[2] = F[4 * pl + cc];
-                        if (N) f[4] = F[2 * pl + cc];
-                        if (W || S) f[5] = F[7 * pl + cc];
-                        if (E || S) f[6] = (E && S) ? s.corner[0] : F[8 * pl + cc];
-                        if (E || N) f[7] = (E && N) ? s.corner[1] : F[5 * pl + cc];
-                        if (W || N) f[8] = F[6 * pl + cc];
-                        /* lambda_f of a boundary node into its own stage words
-                         * (each word of segments 0..17 has one reader) */
-                        wrote = true;
-#pragma unroll
-                        for (int k = 0; k < 9; k++) {
-                            const int xd = x + cx_of(k), yd = y + cy_of(k);
-                            if (!(xd >= 0 && xd < Nx && yd >= 0 && yd < Ny)) {
-                                const bool corner6 = (k == 8) && E && S;
-                                const bool corner7 = (k == 5) && E && N;
-                                stg[k * RW + col + cx_of(k)] = (corner6 || corner7) ? 0.0 : PIN[opp_of(k) * pl + cc];
-                            }
-                        }
-                    }
-                    double rho = 0.0;
-#pragma unroll
-                    for (int k = 0; k < 9; k++) rho += f[k];
-                    X(XS_RHO) = rho;
-                    X(XS_MX) = f[1] - f[3] + f[5] - f[6] - f[7] + f[8];
-                    X(XS_MY) = f[2] - f[4] + f[5] + f[6] - f[7] - f[8];
-                    /* selector sums in the forward kernel's order */
-                    X(XS_KP) = bgk::aplus(wa[1][1]) + bgk::aplus(wa[1][2]) + bgk::aplus(wa[2][1]) +
-                               bgk::aplus(wa[1][0]) + bgk::aplus(wa[0][1]) + bgk::aplus(wa[2][2]) +
-                               bgk::aplus(wa[2][0]) + bgk::aplus(wa[0][0]) + bgk::aplus(wa[0][2]);
-                    X(XS_KM) = bgk::aminus(wa[1][1]) + bgk::aminus(wa[1][2]) + bgk::aminus(wa[2][1]) +
-                               bgk::aminus(wa[1][0]) + bgk::aminus(wa[0][1]) + bgk::aminus(wa[2][2]) +
-                               bgk::aminus(wa[2][0]) + bgk::aminus(wa[0][0]) + bgk::aminus(wa[0][2]);
-                    X(XS_P0) = wa[1][1];
-                } else {
-                    if (y + 1 < Ny) {
-                        wk[2] = row3(stg + 18 * RW, col, hasL, hasR);
-                        wm[2] = row3(stg + 19 * RW, col, hasL, hasR);
-                    } else {
-                        wk[2] = 0.0;
-                        wm[2] = 0.0;
-                    }
-                    /* boundary g values into this node's own stage words, so
-                     * that all nine pulled g are re-read from the stage */
-                    if (W || E) {
-                        const int ym = S ? y : y - 1, yp = N ? y : y + 1;
-                        if (W) {
-                            sg[1 * RW + col - 1] = s.gW[y];
-                            sg[5 * RW + col - 1] = s.gW[Ny + ym];
-                            sg[8 * RW + col - 1] = s.gW[2 * Ny + yp];
-                        }
-                        if (E) {
-                            sg[3 * RW + col + 1] = c.w[3] * s.tcol[y] * s.pE[y];
-                            sg[6 * RW + col + 1] = c.w[6] * s.tcol[ym] * s.pE[Ny + ym];
-                            sg[7 * RW + col + 1] = c.w[7] * s.tcol[yp] * s.pE[2 * Ny + yp];
-                        }
-                    }
-                    if (W || E || S || N) {
-                        wrote = true;
-#pragma unroll
-                        for (int k = 0; k < 9; k++) {
-                            const int xd = x + cx_of(k), yd = y + cy_of(k);
-                            double *wg = stg + (9 + k) * RW + col + cx_of(k);
-                            double a = 0.0;
-                            if (xd >= 0 && xd < Nx) {
-                                if (yd >= 0 && yd < Ny) a += *wg;
-                                if (cy_of(k) == 1 && S) a += PIN[(9 + k) * pl + xd];
-                                if (cy_of(k) == -1 && N) a += PIN[(9 + k) * pl + (long long)(Ny - 1) * P + xd];
-                            }
-                            *wg = a;
-                        }
-                    }
-                    double T = 0.0;
-#pragma unroll
-                    for (int k = 0; k < 9; k++) T += sg[k * RW + col - cx_of(k)];
-                    X(XS_T) = T;
-                    skp = wk[0] + wk[1] + wk[2] + (S ? wk[1] : 0.0) + (N ? wk[1] : 0.0);
-                    skm = wm[0] + wm[1] + wm[2] + (S ? wm[1] : 0.0) + (N ? wm[1] : 0.0);
-                    d0 = stg[20 * RW + col];
-                    double lT = 0.0;
-                    if (E) {
-                        lT += PIN[(9 + 3) * pl + cc] * c.w[3] * s.pE[y];
-                        double a6 = 0.0, a7 = 0.0;
-                        if (y + 1 < Ny) a6 += PIN[(9 + 6) * pl + cc + P];
-                        if (y == 0) a6 += PIN[(9 + 6) * pl + x];
-                        if (y - 1 >= 0) a7 += PIN[(9 + 7) * pl + cc - P];
-                        if (y == Ny - 1) a7 += PIN[(9 + 7) * pl + (long long)(Ny - 1) * P + x];
-                        lT += a6 * c.w[6] * s.pE[Ny + y] + a7 * c.w[7] * s.pE[2 * Ny + y];
-                    }
-                    hT = 0.5 * lT;
-                    if (W) s.gtin[y] += tin_partial(PIN, pl, P, Ny, s.dgW, y);
-                }
-            }
-            if (lane == 0) okx[flow ? 0 : 1] = got ? 1 : 0;
-            pair_sync();
-            if (!(okx[0] && okx[1])) {
-                if (flow && lane == 0) atomicExch(errflag, 13);
-                failed = true;
-            }
-            double axx = 0.0, ayy = 0.0, axy = 0.0;        /* pxxb.. (flow) or txxb.. (thermal) */
-            if (!failed && active) {
-                /* ---- forward chain (both warps) ---- */
-                const double rho = X(XS_RHO), mx = X(XS_MX), my = X(XS_MY);
-                const double kp = X(XS_KP), km = X(XS_KM), p0 = X(XS_P0), T = X(XS_T);
-                const double irho = 1.0 / rho;
-                const double u = irho * mx, v = irho * my;
-                const double th = tanh_sel(((T - c.T_crit) - c.T_act) * s.inv_T_width, s.tanh_mode);
-                const double rp = 0.5 * (1.0 + th), rm = 0.5 * (1.0 - th);
-                const double KP = (kp / 8.0) * rp, KM = (km / 8.0) * rm;
-                const double phn = p0 + (c.f_plus * KP * (1.0 - p0) - c.f_minus * KM * (1.0 + p0));
-                const double Tf = T - c.dts * (phn - p0) / 2.0;
-                const double gb = c.grav * c.beta;
-                const double onep = 1.0 + phn / 2.0;
-                const double omp = 1.0 - phn;
-                const double FX = -(u * omp * 0.5);
-                const double FY = rho * gb * Tf * onep - v * omp * 0.5;
-                const double iorho = 1.0 / (c.omega_f * rho);
-                const double uf = u + FX * iorho, vf = v + FY * iorho;
-                const double *lam = stg + col;
-
-                /* ---- own half of the collision VJP, second exchange ---- */
-                double ub_part = 0.0, vb_part = 0.0, sb_part = 0.0;
-                if (flow) {
-                    const double cf = 1.0 - c.omega_f;
-#pragma unroll
-                    for (int k = 0; k < 9; k++) {
-                        const double A = d_AisQ[k] ? q : m, B = d_BisQ[k] ? q : m;
-                        const double sf = lam[k * RW + cx_of(k)] * cf * c.C[k];
-                        axx += sf * A; ayy += sf * B; axy += 2.0 * sf * d_E[k];
-                    }
-#pragma unroll
-                    for (int j = 0; j < 9; j++) {
-                        const double A = d_AisQ[j] ? q : m, B = d_BisQ[j] ? q : m;
-                        const double db = A * axx + B * ayy + d_E[j] * axy;
-                        const double feqb = lam[j * RW + cx_of(j)] - db;
-                        double du, dv;
-                        const double Pj = poly_k(j, uf, vf, du, dv);
-                        sb_part += feqb * c.w[j] * Pj;
-                        const double Pb = c.w[j] * (feqb * rho);
-                        ub_part += Pb * du;
-                        vb_part += Pb * dv;
-                    }
-                    X(XS_UFB_F) = ub_part; X(XS_VFB_F) = vb_part; X(XS_RHOB_F) = sb_part;
-                } else {
-                    const double cg = 1.0 - c.omega_g;
-                    double txx = 0.0, tyy = 0.0, txy = 0.0;
-#pragma unroll
-                    for (int k = 0; k < 9; k++) {
-                        double du, dv;
-                        const double e = sg[k * RW + col - cx_of(k)] - c.w[k] * Tf * poly_k(k, uf, vf, du, dv);
-                        txx += (d_AisQ[k] ? q : m) * e;
-                        tyy += (d_BisQ[k] ? q : m) * e;
-                        txy += d_E[k] * e;
-                    }
-                    double omg_b = 0.0;
-#pragma unroll
-                    for (int k = 0; k < 9; k++) {
-                        const double A = d_AisQ[k] ? q : m, B = d_BisQ[k] ? q : m;
-                        const double Gob = lam[(9 + k) * RW + cx_of(k)] + hT;
-                        const double Sg = A * txx + B * tyy + 2.0 * d_E[k] * txy;
-                        omg_b += Gob * (-c.C[k] * Sg);
-                        const double sb = Gob * cg * c.C[k];
-                        axx += sb * A; ayy += sb * B; axy += 2.0 * sb * d_E[k];
-                    }
-                    omg_sum += omg_b;
-#pragma unroll
-                    for (int j = 0; j < 9; j++) {
-                        const double A = d_AisQ[j] ? q : m, B = d_BisQ[j] ? q : m;
-                        const double eb = A * axx + B * ayy + d_E[j] * axy;
-                        const double geqb = (lam[(9 + j) * RW + cx_of(j)] + hT) - eb;
-                        double du, dv;
-                        const double Pj = poly_k(j, uf, vf, du, dv);
-                        sb_part += geqb * c.w[j] * Pj;
-                        const double Pb = c.w[j] * (geqb * Tf);
-                        ub_part += Pb * du;
-                        vb_part += Pb * dv;
-                    }
-                    X(XS_UFB_G) = ub_part; X(XS_VFB_G) = vb_part; X(XS_TFB_G) = sb_part;
-                    X(XS_PHNB) = d0 + 0.5 * (1.0 + phn) * skp - 0.5 * (1.0 - phn) * skm;
-                    X(XS_HT) = hT;
-                }
-            }
-            /* the second barrier is taken by every lane of both warps (the
-             * same barrier instruction for the whole warp) */
-            if (!failed) pair_sync();
-            if (!failed && active) {
-                /* the forward chain again, from the exchanged scalars */
-                const double rho = X(XS_RHO), mx = X(XS_MX), my = X(XS_MY);
-                const double kp = X(XS_KP), km = X(XS_KM), p0 = X(XS_P0), T = X(XS_T);
-                const double irho = 1.0 / rho;
-                const double u = irho * mx, v = irho * my;
-                const double th = tanh_sel(((T - c.T_crit) - c.T_act) * s.inv_T_width, s.tanh_mode);
-                const double rp = 0.5 * (1.0 + th), rm = 0.5 * (1.0 - th);
-                const double KP = (kp / 8.0) * rp, KM = (km / 8.0) * rm;
-                const double phn = p0 + (c.f_plus * KP * (1.0 - p0) - c.f_minus * KM * (1.0 + p0));
-                const double Tf = T - c.dts * (phn - p0) / 2.0;
-                const double gb = c.grav * c.beta;
-                const double onep = 1.0 + phn / 2.0;
-                const double omp = 1.0 - phn;
-                const double FX = -(u * omp * 0.5);
-                const double FY = rho * gb * Tf * onep - v * omp * 0.5;
-                const double iorho = 1.0 / (c.omega_f * rho);
-                /* ---- scalar reverse tail (both warps) ---- */
-                const double ufb = X(XS_UFB_F) + X(XS_UFB_G), vfb = X(XS_VFB_F) + X(XS_VFB_G);
-                double rhob = X(XS_RHOB_F), Tfb = X(XS_TFB_G);
-                double ub = ufb, vb = vfb;
-                const double FXb = ufb * iorho, FYb = vfb * iorho;
-                rhob += c.omega_f * (-(ufb * FX + vfb * FY) * (iorho * iorho));
-                vb += -0.5 * omp * FYb;
-                double phnb = 0.5 * v * FYb;
-                ub += -0.5 * omp * FXb;
-                phnb += 0.5 * u * FXb;
-                rhob += FYb * gb * Tf * onep;
-                Tfb += FYb * rho * gb * onep;
-                phnb += FYb * rho * gb * Tf * 0.5;
-                double Tb = Tfb;
-                phnb += -0.5 * c.dts * Tfb;
-                const double PHb = X(XS_PHNB) + phnb;
-                const double KPb = PHb * c.f_plus * (1.0 - p0);
-                const double KMb = -PHb * c.f_minus * (1.0 + p0);
-                double *po = s.pout + cc;
-                if (flow) {
-                    const double mxb = ub * irho, myb = vb * irho;
-                    rhob += -(ub * mx + vb * my) * irho * irho;
-#pragma unroll
-                    for (int j = 0; j < 9; j++) {
-                        const double A = d_AisQ[j] ? q : m, B = d_BisQ[j] ? q : m;
-                        const double db = A * axx + B * ayy + d_E[j] * axy;
-                        po[j * pl] = db + (rhob + cx_of(j) * mxb + cy_of(j) * myb);
-                    }
-                    po[18 * pl] = KPb * rp / 8.0;
-                    po[19 * pl] = KMb * rm / 8.0;
-                } else {
-                    const double thb = 0.5 * (KPb * kp / 8.0) - 0.5 * (KMb * km / 8.0);
-                    Tb += thb * (1.0 - th * th) * s.inv_T_width;
-                    Tb += X(XS_HT);
-#pragma unroll
-                    for (int j = 0; j < 9; j++) {
-                        const double A = d_AisQ[j] ? q : m, B = d_BisQ[j] ? q : m;
-                        const double eb = A * axx + B * ayy + d_E[j] * axy;
-                        po[(9 + j) * pl] = eb + Tb;
-                    }
-                    po[20 * pl] = 0.5 * c.dts * Tfb + PHb * (1.0 - c.f_plus * KP - c.f_minus * KM);
-                }
-            }
-            if (active) {
-                if (flow) {
-#pragma unroll
-                    for (int k = 0; k < 3; k++) {
-                        wa[0][k] = wa[1][k];
-                        wa[1][k] = wa[2][k];
-                    }
-                } else {
-                    wk[0] = wk[1]; wk[1] = wk[2];
-                    wm[0] = wm[1]; wm[1] = wm[2];
-                }
-            }
-            if (__any_sync(0xffffffffu, wrote)) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&empty[st]);
-            r++;
-            ok = it.next();
-            if (failed) break;
-        } while (ok && it.t == tile);
-    }
-    if (!flow) {
-        omg_sum = warp_total(omg_sum);
-        if (lane == 0) s.omg_acc[blockIdx.x * PAIRS + pair] += omg_sum;
-    }
-}
-
 /* Tile height for the reverse step: the H that minimises the waves of tiles
  * times (H + 1), the 1 standing for the per-tile window prologue. */
 PipeSched adj_sched(const bgk_ctx *c, int ctas_per_sm, int bx, int *grid)
@@ -1241,6 +806,7 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
         (void)cudaGetLastError();
         return bgk_internal_fail(BGK_ERR_CUDA, "cudaMemGetInfo failed");
     }
+    free_b += c->adj_ws_bytes;            /* a cached workspace can be given back */
     const size_t margin = (size_t)1 << 30;
     const size_t avail = free_b > fixed_bytes + margin ? free_b - fixed_bytes - margin : 0;
     bool binomial = spec->checkpoint_every < 0 || (size_t)(nsnap + K + 1) * state_bytes > avail;
@@ -1252,56 +818,70 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
             return bgk_internal_fail(BGK_ERR_OOM, "not enough device memory for the adjoint's checkpoints");
     }
 
-    std::vector<void *> allocs;
-    auto dmalloc = [&](size_t bytes) -> double * {
-        void *p = nullptr;
-        if (cudaMalloc(&p, bytes) != cudaSuccess) { (void)cudaGetLastError(); return nullptr; }
-        allocs.push_back(p);
-        return (double *)p;
-    };
-    auto cleanup = [&]() { for (void *p : allocs) cudaFree(p); };
-    /* sqrt(N): nsnap snapshots + K+1 segment states; binomial: nslots slots
-     * + 3 work states.  State i of a block at base + i * state_elems. */
-    const size_t nstates_a = binomial ? (size_t)nslots : (size_t)nsnap;
-    const size_t nstates_b = binomial ? 3 : (size_t)(K + 1);
-    double *blk_a_raw = dmalloc(nstates_a * state_bytes);
-    double *blk_b_raw = dmalloc(nstates_b * state_bytes);
-    double *snaps = blk_a_raw ? blk_a_raw + state_guard : nullptr;
-    double *seg = blk_b_raw ? blk_b_raw + state_guard : nullptr;
-    /* partial planes Pi, guarded like the states (the pipelined reverse step
-     * copies row segments of them) */
-    double *pi_raw[2] = {dmalloc(((size_t)NPI * pl + 2 * state_guard) * sizeof(double)),
-                         dmalloc(((size_t)NPI * pl + 2 * state_guard) * sizeof(double))};
-    double *pi[2] = {pi_raw[0] ? pi_raw[0] + state_guard : nullptr, pi_raw[1] ? pi_raw[1] + state_guard : nullptr};
-    /* reverse-step kernel: 0 = register gather (adj_step_kernel),
-     * 1 = pipeline with one warp per 32 nodes (adj_pipe_kernel),
-     * 2, 3, 4 = warp pairs (adj_pair_kernel) with 4 pairs x 2 CTAs/SM,
-     * 2 pairs x 3 CTAs/SM, 2 pairs x 4 CTAs/SM */
-    int akind = c->tune_pipe ? 1 : 0;
-    if (const char *v = getenv("BGK_ADJ_KERNEL")) akind = atoi(v);
-    if (akind < 0 || akind > 4) akind = 2;
+    /* reverse-step kernel: the shared-memory pipeline (adj_pipe_kernel), or
+     * the register gather (adj_step_kernel) when the context selects the
+     * register-pull kernels */
+    const int akind = c->tune_pipe ? 1 : 0;
     dim3 blk(AB_X, AB_Y), grd((c->Nx + AB_X - 1) / AB_X, (Ny + AB_Y - 1) / AB_Y);
     int pgrid = 0, partials = 0;
     PipeSched psch{};
-    switch (akind) {
-    case 1: psch = adj_sched(c, ADJ_CTAS, PIPE_BX, &pgrid); partials = PIPE_CWARPS; break;
-    case 2: psch = adj_sched(c, 2, PairGeom<4>::BX, &pgrid); partials = 4; break;
-    case 3: psch = adj_sched(c, 3, PairGeom<2>::BX, &pgrid); partials = 2; break;
-    case 4: psch = adj_sched(c, 4, PairGeom<2>::BX, &pgrid); partials = 2; break;
-    default: break;
+    if (akind == 1) {
+        psch = adj_sched(c, ADJ_CTAS, PIPE_BX, &pgrid);
+        partials = PIPE_CWARPS;
     }
     const int nblk = akind ? pgrid * partials : (int)(grd.x * grd.y);
-    double *omg_acc = dmalloc((size_t)nblk * sizeof(double));
-    double *dgW = dmalloc(3 * (size_t)Ny * sizeof(double));
-    double *gtin = dmalloc((size_t)Ny * sizeof(double));
-    double *scal = dmalloc(4 * sizeof(double));
-    int *dpi = (int *)dmalloc((size_t)spec->nprobes * sizeof(int) + 16);
-    int *dpj = (int *)dmalloc((size_t)spec->nprobes * sizeof(int) + 16);
-    double *dtg = dmalloc((size_t)spec->nprobes * sizeof(double));
-    if (!snaps || !seg || !pi[0] || !pi[1] || !omg_acc || !dgW || !gtin || !scal || !dpi || !dpj || !dtg) {
-        cleanup();
-        return bgk_internal_fail(BGK_ERR_OOM, "adjoint workspace allocation failed");
+
+    /* Workspace: one device allocation, carved in 256-byte aligned pieces.
+     * It stays in the context for the next call (freed by bgk_destroy)
+     * unless it is larger than a quarter of the device memory.
+     * sqrt(N): nsnap snapshots + K+1 segment states; binomial: nslots slots
+     * + 3 work states.  State i of a block at base + i * state_elems. */
+    const size_t nstates_a = binomial ? (size_t)nslots : (size_t)nsnap;
+    const size_t nstates_b = binomial ? 3 : (size_t)(K + 1);
+    const size_t pi_bytes = ((size_t)NPI * pl + 2 * state_guard) * sizeof(double);
+    const size_t piece[] = {nstates_a * state_bytes, nstates_b * state_bytes, pi_bytes, pi_bytes,
+                            (size_t)nblk * sizeof(double), 3 * (size_t)Ny * sizeof(double),
+                            (size_t)Ny * sizeof(double), 4 * sizeof(double),
+                            (size_t)spec->nprobes * sizeof(int) + 16, (size_t)spec->nprobes * sizeof(int) + 16,
+                            (size_t)spec->nprobes * sizeof(double)};
+    constexpr int NPIECE = (int)(sizeof(piece) / sizeof(piece[0]));
+    size_t off[NPIECE], ws_bytes = 0;
+    for (int i = 0; i < NPIECE; i++) {
+        off[i] = ws_bytes;
+        ws_bytes += (piece[i] + 255) / 256 * 256;
     }
+    if (c->adj_ws_bytes < ws_bytes) {
+        if (c->adj_ws) cudaFree(c->adj_ws);
+        c->adj_ws = nullptr;
+        c->adj_ws_bytes = 0;
+        if (cudaMalloc(&c->adj_ws, ws_bytes) != cudaSuccess) {
+            (void)cudaGetLastError();
+            c->adj_ws = nullptr;
+            return bgk_internal_fail(BGK_ERR_OOM, "adjoint workspace allocation failed");
+        }
+        c->adj_ws_bytes = ws_bytes;
+    }
+    auto cleanup = [&]() {
+        if (c->adj_ws_bytes > total_b / 4) {
+            cudaFree(c->adj_ws);
+            c->adj_ws = nullptr;
+            c->adj_ws_bytes = 0;
+        }
+    };
+    char *wsb = static_cast<char *>(c->adj_ws);
+    auto at = [&](int i) { return static_cast<void *>(wsb + off[i]); };
+    double *snaps = static_cast<double *>(at(0)) + state_guard;
+    double *seg = static_cast<double *>(at(1)) + state_guard;
+    /* partial planes Pi, guarded like the states (the pipelined reverse step
+     * copies row segments of them) */
+    double *pi[2] = {static_cast<double *>(at(2)) + state_guard, static_cast<double *>(at(3)) + state_guard};
+    double *omg_acc = static_cast<double *>(at(4));
+    double *dgW = static_cast<double *>(at(5));
+    double *gtin = static_cast<double *>(at(6));
+    double *scal = static_cast<double *>(at(7));
+    int *dpi = static_cast<int *>(at(8));
+    int *dpj = static_cast<int *>(at(9));
+    double *dtg = static_cast<double *>(at(10));
 #define ACK(call)                                                                   \
     do {                                                                            \
         cudaError_t e_ = (call);                                                    \
@@ -1336,29 +916,17 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
         a.inv_T_width = 1.0 / c->c.T_width;
         a.plane = pl; a.P = c->P;
         a.tanh_mode = c->opt.tanh_mode;
-        switch (akind) {
-        case 1: adj_pipe_kernel<<<pgrid, PIPE_THREADS, ADJ_SMEM, st>>>(a, c->c, psch, c->errflag); break;
-        case 2:
-            adj_pair_kernel<4, 2><<<pgrid, PairGeom<4>::THREADS, PairGeom<4>::SMEM, st>>>(a, c->c, psch, c->errflag);
-            break;
-        case 3:
-            adj_pair_kernel<2, 3><<<pgrid, PairGeom<2>::THREADS, PairGeom<2>::SMEM, st>>>(a, c->c, psch, c->errflag);
-            break;
-        case 4:
-            adj_pair_kernel<2, 4><<<pgrid, PairGeom<2>::THREADS, PairGeom<2>::SMEM, st>>>(a, c->c, psch, c->errflag);
-            break;
-        default: adj_step_kernel<<<grd, blk, 0, st>>>(a, c->c); break;
-        }
+        if (akind == 1)
+            adj_pipe_kernel<<<pgrid, PIPE_THREADS, ADJ_SMEM, st>>>(a, c->c, psch, c->errflag);
+        else
+            adj_step_kernel<<<grd, blk, 0, st>>>(a, c->c);
         pin ^= 1;
         return cudaGetLastError();
     };
 
-    {
-        static std::atomic<unsigned long long> done1{0}, done2{0}, done3{0}, done4{0};
-        if (akind == 1) ACK(pipe_configure(adj_pipe_kernel, ADJ_SMEM, c->dev, done1));
-        if (akind == 2) ACK(pipe_configure(adj_pair_kernel<4, 2>, PairGeom<4>::SMEM, c->dev, done2));
-        if (akind == 3) ACK(pipe_configure(adj_pair_kernel<2, 3>, PairGeom<2>::SMEM, c->dev, done3));
-        if (akind == 4) ACK(pipe_configure(adj_pair_kernel<2, 4>, PairGeom<2>::SMEM, c->dev, done4));
+    if (akind == 1) {
+        static std::atomic<unsigned long long> done{0};
+        ACK(pipe_configure(adj_pipe_kernel, ADJ_SMEM, c->dev, done));
     }
     ACK(cudaMemcpyAsync(dpi, spec->probe_i, spec->nprobes * sizeof(int), cudaMemcpyHostToDevice, st));
     ACK(cudaMemcpyAsync(dpj, spec->probe_j, spec->nprobes * sizeof(int), cudaMemcpyHostToDevice, st));

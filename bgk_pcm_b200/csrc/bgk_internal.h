@@ -137,6 +137,8 @@ struct bgk_ctx {
      * pulls; pipeline depth and CTAs per SM (BGK_PIPE, BGK_PIPE_D,
      * BGK_PIPE_CTAS) */
     int tune_pipe, tune_D, tune_ctas, nsm;
+    void *adj_ws;          /* adjoint workspace kept between bgk_adjoint_run calls */
+    size_t adj_ws_bytes;
 };
 
 namespace bgk {

@@ -484,6 +484,7 @@ int bgk_destroy(bgk_ctx *c)
         if (c->sgp[k]) cudaFree(c->sgp[k]);
     }
     if (c->pinned) cudaFreeHost(c->pinned);
+    if (c->adj_ws) cudaFree(c->adj_ws);
     free(c->tin_host);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;

@@ -205,7 +205,9 @@ typedef struct bgk_adjoint_spec {
  * reference counterpart (the reference has no derivatives).  Requires an FP64
  * context created with opt.smooth = 1 (the differentiable form).  The
  * context is left at the final state, exactly as bgk_step(ctx, nsteps)
- * leaves it.  grad_tin may be NULL. */
+ * leaves it.  grad_tin may be NULL.  The workspace (snapshots, recompute
+ * buffer, partials) stays allocated in the context for the next call unless
+ * it exceeds a quarter of the device memory; bgk_destroy frees it. */
 int bgk_adjoint_run(bgk_ctx *ctx, const bgk_adjoint_spec *spec, double *loss,
                     double *grad_tin, double *grad_tau_g);
 

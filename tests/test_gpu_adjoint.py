@@ -77,6 +77,22 @@ def test_adjoint_binomial_schedule_matches_sqrt_schedule(lib, slots):
     np.testing.assert_array_equal(a[1], b[1])
 
 
+def test_adjoint_repeated_on_one_context(lib):
+    """The workspace kept in the context between calls (and its stale
+    contents) does not change the result; a larger second call regrows it."""
+    from bgk_pcm_b200 import Solver, gradcheck as gc
+    p, tin, tin_t, pi, pj = gc.setup(Nx=40, Ny=33, steps=30, nprobes=10, **SENSITIVE)
+    target = gc.forward_phi(p, tin_t, 30, pi, pj)
+    ref = gc.adjoint(p, tin, 30, pi, pj, target, checkpoint_every=6)
+    with Solver(p, smooth=True) as s:
+        for K in (6, 30, 6):
+            s.initialization()
+            s.set_tin(tin)
+            out = s.adjoint(30, pi, pj, target, K)
+            assert out[0] == ref[0] and out[2] == ref[2]
+            np.testing.assert_array_equal(out[1], ref[1])
+
+
 @pytest.mark.slow
 def test_adjoint_config4_fd_16_directions(lib):
     """512x512, Ra 1e5, 2000 steps, 64 probes, checkpoints every 45 steps:
