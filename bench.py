@@ -109,10 +109,11 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_oracle_rate(params, budget_s: float = 15.0, max_steps: int = 400):
-    """GLUPS of the CPU oracle (all host threads) on whole steps of `params`."""
+def cpu_oracle_rate(params, budget_s: float = 15.0, max_steps: int = 400, threads: int = 0):
+    """GLUPS of the CPU oracle on whole steps of `params`, with `threads`
+    OpenMP threads (0: all host threads; 1: the serial STEP_7 restatement)."""
     from oracle import pyoracle
-    threads = os.cpu_count() or 1
+    threads = threads or os.cpu_count() or 1
     o = pyoracle.Oracle(params, threads=threads)
     o.initialization()
     t0 = time.perf_counter()
@@ -134,6 +135,22 @@ def load_traffic(kernel_key: str):
         return None
     d = json.loads(f.read_text())
     return d.get(kernel_key, {}).get("traffic_bytes_per_launch")
+
+
+def max_over_ranks(value: float, dist, device) -> float:
+    """The maximum of `value` over all ranks (the job's time is its slowest
+    rank's); `dist` is None for a single process."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_glups(nodes: int, steps: int, world: int, ms_max: float) -> float:
+    """Node updates of all ranks (each runs its own replica) per second."""
+    return nodes * steps * world / (ms_max / 1e3) / 1e9
 
 
 def time_steps(solver, steps: int, torch):
@@ -298,11 +315,8 @@ def main():
         return ms, clocks
 
     ms, clocks = run_form(args.precision, False, args.steps, args.warmup, sample_clocks=True)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = nodes * args.steps * world / (ms / 1e3) / 1e9
+    ms = max_over_ranks(ms, dist, "cuda")
+    value = whole_job_glups(nodes, args.steps, world, ms)
     hbm, hbm_kind = peaks()
     bpn = BYTES_PER_NODE[args.precision]
     achieved = bpn * nodes / (ms / 1e3 / args.steps) / 1e9
@@ -310,7 +324,9 @@ def main():
     traffic = load_traffic(kernel_key)
 
     forms = {}
-    for form in [f for f in args.forms.split(",") if f and f != "none"]:
+    # extra forms on a single process only: a form that fails on one rank
+    # must not leave the ranks at different collective steps
+    for form in [f for f in args.forms.split(",") if f and f != "none" and world == 1]:
         prec, fma = ("f64", True) if form == "f64fma" else (form, False)
         try:
             fms, _ = run_form(prec, fma, max(args.steps // 4, 100), args.warmup)
@@ -329,21 +345,21 @@ def main():
     e2e = None
     if not args.no_e2e:
         e_ms, h2d, d2h = e2e_run(params, args.precision, args.steps, local, torch)
-        if dist:
-            t = torch.tensor([e_ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_ms = float(t.item())
-        e2e = {"value": nodes * args.steps * world / (e_ms / 1e3) / 1e9, "unit": "GLUPS",
+        e_ms = max_over_ranks(e_ms, dist, "cuda")
+        e2e = {"value": whole_job_glups(nodes, args.steps, world, e_ms), "unit": "GLUPS",
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                "what": "initial state (23 reference-layout fields) uploaded from pinned host memory, the steps "
                        "with field sums + probe read back every 1000 steps, final rho/T/u/v/phi downloaded"}
 
-    cpu = None
+    cpu = cpu1 = None
     if rank == 0 and world == 1 and not args.no_cpu:
         glups, n, threads = cpu_oracle_rate(params)
         cpu = {"value": glups, "unit": "GLUPS", "cores": threads, "kind": "port",
                "sample": f"{n} whole steps of the {Nx}x{Ny} grid, C restatement of STEP_7 with OpenMP "
-                         "(bit-identical to serial)"}
+                         "(STEP_OPENMP's parallelisation; bit-identical to serial)"}
+        glups1, n1, _ = cpu_oracle_rate(params, budget_s=8.0, threads=1)
+        cpu1 = {"value": glups1, "unit": "GLUPS", "cores": 1, "kind": "port",
+                "sample": f"{n1} whole steps of the {Nx}x{Ny} grid, serial C restatement of STEP_7"}
 
     if rank == 0:
         line = {
@@ -364,6 +380,7 @@ def main():
             "clocks": clocks,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "cpu_baseline_serial": cpu1,
             "gpu_launches": args.steps + 1,
         }
         print(json.dumps(line), flush=True)
