@@ -396,9 +396,10 @@ constexpr int ADJ_SEG_BYTES = ADJ_RW * (int)sizeof(double);
 constexpr int ADJ_NSEG = 40;
 constexpr int ADJ_STAGE_BYTES = ADJ_NSEG * ADJ_SEG_BYTES;
 constexpr int ADJ_HEADER = 256;
-constexpr int ADJ_D = 2;                                  /* stages */
-constexpr int ADJ_CTAS = 2;                               /* CTAs per SM */
-constexpr size_t ADJ_SMEM = (size_t)ADJ_HEADER + (size_t)ADJ_D * ADJ_STAGE_BYTES;
+/* stages D and CTAs per SM: (2, 2) keeps a stage in flight while the
+ * consumers work (168 registers); (1, 3) trades that for 50 % more warps
+ * (128 registers) */
+__host__ __device__ constexpr size_t adj_smem(int D) { return (size_t)ADJ_HEADER + (size_t)D * ADJ_STAGE_BYTES; }
 
 __host__ __device__ constexpr int opp_of(int k) { return k == 0 ? 0 : (k <= 4 ? (k + 1) % 4 + 1 : (k + 1) % 4 + 5); }
 static_assert(opp_of(1) == 3 && opp_of(2) == 4 && opp_of(3) == 1 && opp_of(4) == 2, "opposites");
@@ -452,6 +453,7 @@ __device__ __forceinline__ double row3(const double *v, int i, bool hasL, bool h
     return (hasL ? v[i - 1] : 0.0) + v[i] + (hasR ? v[i + 1] : 0.0);
 }
 
+template <int ADJ_D, int ADJ_CTAS>
 __global__ void __launch_bounds__(PIPE_THREADS, ADJ_CTAS)
 adj_pipe_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
 {
@@ -825,8 +827,12 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
     dim3 blk(AB_X, AB_Y), grd((c->Nx + AB_X - 1) / AB_X, (Ny + AB_Y - 1) / AB_Y);
     int pgrid = 0, partials = 0;
     PipeSched psch{};
+    /* pipeline depth and CTAs per SM of the reverse step (BGK_ADJ_PIPE=1:
+     * one stage, three CTAs per SM) */
+    int adj_d = 2, adj_ctas = 2;
+    if (const char *v = getenv("BGK_ADJ_PIPE")) if (atoi(v) == 1) { adj_d = 1; adj_ctas = 3; }
     if (akind == 1) {
-        psch = adj_sched(c, ADJ_CTAS, PIPE_BX, &pgrid);
+        psch = adj_sched(c, adj_ctas, PIPE_BX, &pgrid);
         partials = PIPE_CWARPS;
     }
     const int nblk = akind ? pgrid * partials : (int)(grd.x * grd.y);
@@ -917,7 +923,12 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
         a.plane = pl; a.P = c->P;
         a.tanh_mode = c->opt.tanh_mode;
         if (akind == 1)
-            adj_pipe_kernel<<<pgrid, PIPE_THREADS, ADJ_SMEM, st>>>(a, c->c, psch, c->errflag);
+        {
+            if (adj_d == 1)
+                adj_pipe_kernel<1, 3><<<pgrid, PIPE_THREADS, adj_smem(1), st>>>(a, c->c, psch, c->errflag);
+            else
+                adj_pipe_kernel<2, 2><<<pgrid, PIPE_THREADS, adj_smem(2), st>>>(a, c->c, psch, c->errflag);
+        }
         else
             adj_step_kernel<<<grd, blk, 0, st>>>(a, c->c);
         pin ^= 1;
@@ -926,7 +937,9 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
 
     if (akind == 1) {
         static std::atomic<unsigned long long> done{0};
-        ACK(pipe_configure(adj_pipe_kernel, ADJ_SMEM, c->dev, done));
+        static std::atomic<unsigned long long> done1{0};
+        if (adj_d == 1) ACK(pipe_configure(adj_pipe_kernel<1, 3>, adj_smem(1), c->dev, done1));
+        else ACK(pipe_configure(adj_pipe_kernel<2, 2>, adj_smem(2), c->dev, done));
     }
     ACK(cudaMemcpyAsync(dpi, spec->probe_i, spec->nprobes * sizeof(int), cudaMemcpyHostToDevice, st));
     ACK(cudaMemcpyAsync(dpj, spec->probe_j, spec->nprobes * sizeof(int), cudaMemcpyHostToDevice, st));
