@@ -10,7 +10,10 @@ Ra 1e8, Pr 1, Stefan 0.5.
      schedule is chosen by the library: sqrt(N) snapshots when they fit in
      free HBM, else the binomial schedule over as many state slots as fit.
   3. FP64 central differences along `ndir` random unit directions in
-     (theta, tau_g), theta the dimensionless hot-wall temperature, h = 1e-6.
+     (theta, tau_g), theta the dimensionless hot-wall temperature, for step
+     sizes h = 1e-6 and 1e-4 (the difference quotient of a long run carries
+     rounding noise that grows with the run's length; the larger step shows
+     how much of the disagreement at the smaller one is that noise).
 
     python -m bgk_pcm_b200.combined                      # the full workload
     python -m bgk_pcm_b200.combined --nx 512 --ny 128 --steps 2000 --adjoint-steps 200
@@ -86,7 +89,7 @@ def loss_fp64(p, state, it, tin, tau_g, steps, pi, pj) -> float:
 
 
 def run(nx=16384, ny=4096, Ra=1e8, Ste=0.5, steps=50000, adj_steps=5000, ndir=8, nprobes=64, seed=0,
-        h=1e-6, checkpoint_every=0, precision="f32"):
+        h=(1e-6, 1e-4), checkpoint_every=0, precision="f32"):
     p = inputs.workload_params(Nx=nx, Ny=ny, iter=steps, Ra=Ra, Ste=Ste)
     rng = np.random.default_rng(seed)
     out = {"workload": f"cavity{nx}x{ny}_ra{Ra:.0e}_ste{Ste}", "steps": steps, "adjoint_steps": adj_steps}
@@ -122,18 +125,24 @@ def run(nx=16384, ny=4096, Ra=1e8, Ste=0.5, steps=50000, adj_steps=5000, ndir=8,
     out["adjoint"] = {"loss": loss, "seconds": t_adj, "forward_seconds": t_fwd, "ratio": t_adj / t_fwd,
                       "nprobes": int(pi.size), "checkpoint_every": checkpoint_every}
 
-    # 3. FP64 central differences in (theta, tau_g)
-    rows = []
+    # 3. FP64 central differences in (theta, tau_g), the same directions for
+    # every step size h
+    hs = (h,) if np.isscalar(h) else tuple(h)
+    dirs = []
     for _ in range(ndir):
         v = rng.standard_normal(ny + 1)
-        v /= np.linalg.norm(v)
-        vt, vtau = v[:-1], v[-1]
-        lp = loss_fp64(p, state, n0, tin + h * dT * vt, p["tau_g"] + h * vtau, adj_steps, pi, pj)
-        lm = loss_fp64(p, state, n0, tin - h * dT * vt, p["tau_g"] - h * vtau, adj_steps, pi, pj)
-        fd = (lp - lm) / (2 * h)
-        ad = float(dT * (g @ vt) + gtau * vtau)
-        rows.append({"fd": fd, "adjoint": ad, "rel_err": abs(fd - ad) / max(abs(ad), 1e-300)})
-    out["fd"] = {"h": h, "directions": rows, "worst_rel_err": max(r["rel_err"] for r in rows)}
+        dirs.append(v / np.linalg.norm(v))
+    out["fd"] = []
+    for hh in hs:
+        rows = []
+        for v in dirs:
+            vt, vtau = v[:-1], v[-1]
+            lp = loss_fp64(p, state, n0, tin + hh * dT * vt, p["tau_g"] + hh * vtau, adj_steps, pi, pj)
+            lm = loss_fp64(p, state, n0, tin - hh * dT * vt, p["tau_g"] - hh * vtau, adj_steps, pi, pj)
+            fd = (lp - lm) / (2 * hh)
+            ad = float(dT * (g @ vt) + gtau * vtau)
+            rows.append({"fd": fd, "adjoint": ad, "rel_err": abs(fd - ad) / max(abs(ad), 1e-300)})
+        out["fd"].append({"h": hh, "directions": rows, "worst_rel_err": max(r["rel_err"] for r in rows)})
     return out
 
 

@@ -60,6 +60,7 @@ struct AdjPtrs {
     double *omg_acc;                       /* per-block running sums         */
     const double *dgW;                     /* d gW_k / d Tin per row         */
     double inv_T_width;                    /* 1 / T_width                    */
+    double inv_omega_f;                    /* 1 / omega_f = tau_f            */
     double *gtin;                          /* dL/dTin per row                */
     long long plane;
     int P;
@@ -98,7 +99,7 @@ template <class FOB, class GOB, class OUTF, class OUTG>
 __device__ __forceinline__ void node_vjp(const Consts &c, int tanh_mode, const double *f, const double *g, double kp, double km,
                          double p0, FOB Fo_b, GOB Go_b, double d0, double skp, double skm,
                          double Tm_b, OUTF out_fb, OUTG out_gb, double &kp_b, double &km_b, double &p0_b,
-                         double &omg_b, double inv_Tw)
+                         double &omg_b, double inv_Tw, double inv_of)
 {
     const double m = c.m_cs2, q = c.q_cs2;
     /* ---- forward recompute ---- */
@@ -123,7 +124,7 @@ __device__ __forceinline__ void node_vjp(const Consts &c, int tanh_mode, const d
     const double FX = -(u * omp * 0.5);
     const double FY = FY0 - v * omp * 0.5;
     const double orho = c.omega_f * rho;
-    const double iorho = 1.0 / orho;
+    const double iorho = irho * inv_of;   /* 1 / (omega_f rho) */
     const double uf = u + FX * iorho, vf = v + FY * iorho;
     /* non-equilibrium moments of g; the polynomials P_k(uf, vf) and their
      * gradients are formed per k where they are used (fewer live registers) */
@@ -350,7 +351,7 @@ adj_step_kernel(AdjPtrs s, Consts c)
         double fb[9], gbv[9], kpb, kmb, p0b;
         node_vjp(c, s.tanh_mode, f, g, kp, km, ph, [&](int k) { return lf[k]; }, [&](int k) { return lg[k]; }, d0,
                  skp, skm, lT, [&](int k, double v) { fb[k] = v; }, [&](int k, double v) { gbv[k] = v; }, kpb, kmb,
-                 p0b, omg_b, s.inv_T_width);
+                 p0b, omg_b, s.inv_T_width, s.inv_omega_f);
 #pragma unroll
         for (int k = 0; k < 9; k++) {
             s.pout[k * pl + cc] = fb[k];
@@ -662,7 +663,7 @@ adj_pipe_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
                          [&](int k) { return lam[k * ADJ_RW + cx_of(k)]; },
                          [&](int k) { return lam[(9 + k) * ADJ_RW + cx_of(k)]; }, d0, skp, skm, lT,
                          [&](int k, double v) { po[k * pl] = v; }, [&](int k, double v) { po[(9 + k) * pl] = v; },
-                         kpb, kmb, p0b, omg_b, s.inv_T_width);
+                         kpb, kmb, p0b, omg_b, s.inv_T_width, s.inv_omega_f);
                 omg_sum += omg_b;
                 s.pout[18 * pl + cc] = kpb;
                 s.pout[19 * pl + cc] = kmb;
@@ -920,6 +921,7 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
         a.omg_acc = omg_acc;
         a.dgW = dgW; a.gtin = gtin;
         a.inv_T_width = 1.0 / c->c.T_width;
+        a.inv_omega_f = 1.0 / c->c.omega_f;
         a.plane = pl; a.P = c->P;
         a.tanh_mode = c->opt.tanh_mode;
         if (akind == 1)
@@ -956,7 +958,7 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
     } else {
         for (int n0 = 0; n0 < N; n0 += K) {
             const int len = (n0 + K < N) ? K : N - n0;
-            rc = bgk_step(c, len);
+            rc = (n0 + len < N) ? bgk_internal_advance(c, len) : bgk_step(c, len);
             if (rc) { cleanup(); return rc; }
             if (n0 + len < N) ACK(copy_state_in(snaps + (size_t)((n0 + len) / K) * state_elems, c->cur));
         }

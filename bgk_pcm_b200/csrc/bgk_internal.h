@@ -166,5 +166,6 @@ cudaError_t launch_init_lowp(bgk_ctx *c);
 /* capi.cu helpers shared with adjoint.cu */
 int bgk_internal_fail(int code, const char *msg);
 int bgk_internal_prepare_fused(bgk_ctx *c);   /* device, fused state, BC arrays */
+int bgk_internal_advance(bgk_ctx *c, int nsteps); /* fused steps, no mirror writes */
 
 #endif

@@ -330,6 +330,24 @@ int bgk_internal_prepare_fused(bgk_ctx *c)
     return BGK_OK;
 }
 
+/* n fused steps without the reference-layout moments and halos (the
+ * mirrors keep their values from before): the adjoint's forward pass
+ * between snapshots, whose last chunk goes through bgk_step. */
+int bgk_internal_advance(bgk_ctx *c, int nsteps)
+{
+    int rc = bgk_internal_prepare_fused(c);
+    if (rc) return rc;
+    c->pristine = false;
+    const bool exact = c->opt.precision == BGK_PREC_F64 && !c->opt.fma;
+    for (int t = 0; t < nsteps; t++) {
+        if (exact) CK(bgk::launch_fused_f64(c, false), "fused step");
+        else CK(bgk::launch_fused_fast(c, false), "fused step");
+        c->cur ^= 1;
+        c->it += 1;
+    }
+    return BGK_OK;
+}
+
 extern "C" {
 
 const char *bgk_last_error(void) { return g_err; }

@@ -82,6 +82,7 @@ struct ConstsLP {
     AT f_plus, f_minus;
     AT gb;                   /* grav * beta                                  */
     AT omega_f;
+    AT inv_omega_f;          /* 1 / omega_f = tau_f                          */
     /* 1 - sum_k w[k] in exact arithmetic over the rounded weights (-7.45e-9
      * for float).  Added to the k = 0 equilibrium times the density and
      * temperature deviations, so that sum_k feq_k = drho and sum_k geq_k =
@@ -227,7 +228,7 @@ __device__ __forceinline__ void node_lp(const LpPtrs<S, PT> &s, const ConstsLP<A
     const AT omp = (AT)1 - phn;
     const AT forceY = rho * c.gb * T * ((AT)1 + (AT)0.5 * phn) - (AT)0.5 * v * omp;
     const AT forceX = (AT)-0.5 * u * omp;
-    const AT iw = (AT)1 / (c.omega_f * rho);
+    const AT iw = irho * c.inv_omega_f;     /* 1 / (omega_f rho), one division less */
     u = u + forceX * iw;
     v = v + forceY * iw;
 
@@ -622,6 +623,7 @@ ConstsLP<AT> make_lp(const bgk_ctx *b)
     l.f_minus = (AT)c.f_minus;
     l.gb = (AT)(c.grav * c.beta);
     l.omega_f = (AT)c.omega_f;
+    l.inv_omega_f = (AT)(1.0 / c.omega_f);
     {
         double ws = 0.0;   /* exact: nine floats of similar size sum without rounding in double */
         for (int k = 0; k < 9; k++) ws += (double)l.w[k];
