@@ -12,7 +12,10 @@
  * would use is bgk_pcm_b200/fortran/bgk_c.f90).
  *
  * usage: bgk_thermal [dir] [--precision f64|f32|f16|f32x] [--fma] [--tanh portable]
- *                    [--snapshot-in file] [--snapshot-out file]
+ *                    [--snapshot-in file] [--snapshot-out file] [--dump-out]
+ * dump != 0 in input.dat restarts from the reference's text dump
+ * (dumpFile.dat, plus dumpPhi.dat when present); --dump-out writes both at
+ * the end of the run.
  */
 #include <cmath>
 #include <cstdint>
@@ -264,6 +267,113 @@ void out2d(Ctx &c)
     fclose(f);
 }
 
+/* The 22 arrays of the reference's text restart, in the order of one node's
+ * two records (STEP_7/dump_out.f90:10-17). */
+const int kDumpFields[22] = {BGK_FIELD_U, BGK_FIELD_V, BGK_FIELD_RHO,
+                             BGK_FIELD_F0 + 0, BGK_FIELD_F0 + 1, BGK_FIELD_F0 + 2, BGK_FIELD_F0 + 3,
+                             BGK_FIELD_F0 + 4, BGK_FIELD_F0 + 5, BGK_FIELD_F0 + 6, BGK_FIELD_F0 + 7,
+                             BGK_FIELD_F0 + 8, BGK_FIELD_T,
+                             BGK_FIELD_G0 + 0, BGK_FIELD_G0 + 1, BGK_FIELD_G0 + 2, BGK_FIELD_G0 + 3,
+                             BGK_FIELD_G0 + 4, BGK_FIELD_G0 + 5, BGK_FIELD_G0 + 6, BGK_FIELD_G0 + 7,
+                             BGK_FIELD_G0 + 8};
+
+/* gfortran list-directed item: one blank, then the value right-justified in
+ * 25 columns (G25.17E3: F form followed by 5 blanks, or E form). */
+std::string fitem(double x)
+{
+    std::string v = flist(x);
+    if (v.find('E') == std::string::npos) v += "     ";
+    if (v.size() < 25) v = std::string(25 - v.size(), ' ') + v;
+    return " " + v;
+}
+
+/* STEP_7/dump_out.f90: dumpFile.dat with it and, for every node (i fastest,
+ * halos included), u v rho f0..f8 on one record and T g0..g8 on the next.
+ * The reference's file omits phi; it is written to dumpPhi.dat (one value
+ * per record, same node order) so that a restart can restore it. */
+void dump_out(Ctx &c)
+{
+    const int NX2 = c.Nx + 2, NY2 = c.Ny + 2;
+    const size_t A = (size_t)NX2 * NY2;
+    std::vector<double> a(22 * A), phi(A);
+    for (int k = 0; k < 22; k++) CALL(bgk_download(c.h, kDumpFields[k], a.data() + k * A, NX2));
+    CALL(bgk_download(c.h, BGK_FIELD_PHI, phi.data(), NX2));
+    FILE *f = open_unit(c, "dumpFile.dat", "w");
+    fprintf(f, " %11d\n", get_it(c));
+    std::string line;
+    for (size_t q = 0; q < A; q++) {
+        line.clear();
+        for (int k = 0; k < 12; k++) line += fitem(a[k * A + q]);
+        line += "\n";
+        for (int k = 12; k < 22; k++) line += fitem(a[k * A + q]);
+        line += "\n";
+        fputs(line.c_str(), f);
+    }
+    fclose(f);
+    FILE *fp = open_unit(c, "dumpPhi.dat", "w");
+    for (size_t q = 0; q < A; q++) fprintf(fp, "%s\n", fitem(phi[q]).c_str());
+    fclose(fp);
+}
+
+/* Next real of a list-directed file (E or D exponents). */
+bool read_real(FILE *f, double *x)
+{
+    char tok[128];
+    if (fscanf(f, "%127s", tok) != 1) return false;
+    for (char *p = tok; *p; p++)
+        if (*p == 'D' || *p == 'd') *p = 'E';
+    char *end = nullptr;
+    *x = strtod(tok, &end);
+    return end && *end == 0;
+}
+
+/* STEP_7/dump_in.f90 for dump != 0: the state of dumpFile.dat (and phi from
+ * dumpPhi.dat when present) over a fresh initial condition. */
+int dump_in(Ctx &c)
+{
+    const int NX2 = c.Nx + 2, NY2 = c.Ny + 2;
+    const size_t A = (size_t)NX2 * NY2;
+    std::string path = c.dir + "/dumpFile.dat";
+    FILE *f = fopen(path.c_str(), "r");
+    if (!f) {
+        fprintf(stderr, "bgk_thermal: dump = %d but %s cannot be opened\n", c.p.dump, path.c_str());
+        exit(1);
+    }
+    double itd = 0.0;
+    if (!read_real(f, &itd)) {
+        fprintf(stderr, "bgk_thermal: %s: no iteration count\n", path.c_str());
+        exit(1);
+    }
+    std::vector<double> a(22 * A);
+    for (size_t q = 0; q < A; q++)
+        for (int k = 0; k < 22; k++)
+            if (!read_real(f, &a[k * A + q])) {
+                fprintf(stderr, "bgk_thermal: %s ends early (node %zu of %zu)\n", path.c_str(), q, A);
+                exit(1);
+            }
+    fclose(f);
+    CALL(bgk_initialize(c.h));
+    for (int k = 0; k < 22; k++) CALL(bgk_upload(c.h, kDumpFields[k], a.data() + k * A, NX2));
+    std::string ppath = c.dir + "/dumpPhi.dat";
+    FILE *fp = fopen(ppath.c_str(), "r");
+    if (fp) {
+        std::vector<double> phi(A);
+        for (size_t q = 0; q < A; q++)
+            if (!read_real(fp, &phi[q])) {
+                fprintf(stderr, "bgk_thermal: %s ends early\n", ppath.c_str());
+                exit(1);
+            }
+        fclose(fp);
+        CALL(bgk_upload(c.h, BGK_FIELD_PHI, phi.data(), NX2));
+    } else {
+        fprintf(stderr, "bgk_thermal: %s not found: phi keeps the initial condition (the reference's "
+                        "dumpFile.dat does not hold phi)\n", ppath.c_str());
+    }
+    const int it = (int)itd;
+    CALL(bgk_set_it(c.h, it));
+    return it;
+}
+
 double get_mem_mb()
 {
     struct rusage r;
@@ -279,6 +389,7 @@ int main(int argc, char **argv)
     c.dir = ".";
     bgk_options opt{BGK_PREC_F64, BGK_TANH_DEVICE, 0, -1, 0};
     std::string snap_in, snap_out;
+    bool dump_at_end = false;
     for (int a = 1; a < argc; a++) {
         std::string s = argv[a];
         if (s == "--precision" && a + 1 < argc) {
@@ -293,6 +404,8 @@ int main(int argc, char **argv)
             snap_in = argv[++a];
         } else if (s == "--snapshot-out" && a + 1 < argc) {
             snap_out = argv[++a];
+        } else if (s == "--dump-out") {
+            dump_at_end = true;
         } else {
             c.dir = s;
         }
@@ -310,11 +423,9 @@ int main(int argc, char **argv)
     if (!snap_in.empty()) {
         CALL(bgk_load(c.h, snap_in.c_str()));
         it = get_it(c);
+    } else if (c.p.dump != 0) {
+        it = dump_in(c);
     } else {
-        if (c.p.dump != 0)
-            fprintf(stderr, "bgk_thermal: dump = %d: the text restart (dumpFile.dat) does not restore phi in the "
-                            "reference; use --snapshot-in for a complete restart. Starting from the initial "
-                            "condition.\n", c.p.dump);
         CALL(bgk_initialize(c.h));
         FILE *lg = open_unit(c, "log.dat", "w");
         fprintf(lg, " iteration    mass\n ====================\n");
@@ -376,6 +487,7 @@ int main(int argc, char **argv)
     printf("INFO: Memory used (MB)      %14.6f \n", get_mem_mb());
     printf(" ==========================================\n");
     if (!snap_out.empty()) CALL(bgk_save(c.h, snap_out.c_str()));
+    if (dump_at_end) dump_out(c);
     FILE *us[] = {c.u64, c.u69, c.u164, c.u666, c.u667, c.u668};
     for (FILE *f : us) fclose(f);
     CALL(bgk_destroy(c.h));
