@@ -196,8 +196,7 @@ __device__ __forceinline__ double tanh_pt<double>(double x, int mode)
  * stores, moments.  Shared by the register-pull and pipeline kernels. */
 template <typename S, typename PT, typename AT, int TANH, bool MOM>
 __device__ __forceinline__ void node_lp(const LpPtrs<S, PT> &s, const ConstsLP<AT> &c, int x, int y, long long cc,
-                                        bool E, AT *f, AT *g, const PT (&ap)[3][3], const PT (&am)[3][3],
-                                        const PT *pc)
+                                        bool E, AT *f, AT *g, PT kp, PT km, PT p0)
 {
     using C = Codec<S>;
     const long long pl = s.plane;
@@ -214,9 +213,6 @@ __device__ __forceinline__ void node_lp(const LpPtrs<S, PT> &s, const ConstsLP<A
     /* phase_field (in PT) */
     const PT one = (PT)1, half = (PT)0.5;
     const PT th = tanh_pt<PT>(((PT)c.T0mTcrit_d + (PT)dT) * (PT)c.inv_T_width_d, TANH);
-    const PT kp = ap[1][1] + ap[1][2] + ap[2][1] + ap[1][0] + ap[0][1] + ap[2][2] + ap[2][0] + ap[0][0] + ap[0][2];
-    const PT km = am[1][1] + am[1][2] + am[2][1] + am[1][0] + am[0][1] + am[2][2] + am[2][0] + am[0][0] + am[0][2];
-    const PT p0 = pc[1];
     const PT kpp = kp * (PT)0.125 * (half * (one + th));
     const PT kmm = km * (PT)0.125 * (half * (one - th));
     const PT phn_p = p0 + (half * kpp * (one - p0) - half * kmm * (one + p0));
@@ -290,7 +286,7 @@ fused_lowp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, int H, int pf)
     const PT *__restrict__ PH = s.phin;
     const float isf = s.inv_sf, isg = s.inv_sg;
 
-    PT ap[3][3], am[3][3], pc[3];
+    PT ap[3], am[3], pc[3];   /* per row y-1, y, y+1: sums over x-1..x+1 of (1/2 (1 +- phi))^2, and phi */
     auto load_row = [&](int r, int slot) {
         const int rc = r < 0 ? 0 : (r >= Ny ? Ny - 1 : r);
         const PT *row = PH + (long long)rc * P;
@@ -300,8 +296,8 @@ fused_lowp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, int H, int pf)
         const PT h = (PT)0.5, one = (PT)1;
         const PT a0 = h * (one + pL), a1 = h * (one + pM), a2 = h * (one + pR);
         const PT b0 = h * (one - pL), b1 = h * (one - pM), b2 = h * (one - pR);
-        ap[slot][0] = a0 * a0; ap[slot][1] = a1 * a1; ap[slot][2] = a2 * a2;
-        am[slot][0] = b0 * b0; am[slot][1] = b1 * b1; am[slot][2] = b2 * b2;
+        ap[slot] = a0 * a0 + a1 * a1 + a2 * a2;
+        am[slot] = b0 * b0 + b1 * b1 + b2 * b2;
         pc[slot] = pM;
     };
     load_row(y0 - 1, 0);
@@ -351,13 +347,10 @@ fused_lowp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, int H, int pf)
             g[7] = (AT)C::ld(G + 7 * pl + cp + 1, isg);
         }
 
-        node_lp<S, PT, AT, TANH, MOM>(s, c, x, y, cc, E, f, g, ap, am, pc);
+        node_lp<S, PT, AT, TANH, MOM>(s, c, x, y, cc, E, f, g, (ap[0] + ap[1]) + ap[2], (am[0] + am[1]) + am[2], pc[1]);
 
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-            ap[0][k] = ap[1][k]; ap[1][k] = ap[2][k];
-            am[0][k] = am[1][k]; am[1][k] = am[2][k];
-        }
+        ap[0] = ap[1]; ap[1] = ap[2];
+        am[0] = am[1]; am[1] = am[2];
         pc[0] = pc[1]; pc[1] = pc[2];
     }
 }
@@ -417,7 +410,7 @@ fused_pipe_lp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, PipeSched sch, int *errfla
         const int x = it.x0 + tid;
         const bool active = x < Nx;
         const bool W = (x == 0), E = (x == Nx - 1);
-        PT ap[3][3], am[3][3], pc[3];
+        PT ap[3], am[3], pc[3];   /* per row y-1, y, y+1: sums over x-1..x+1 of (1/2 (1 +- phi))^2, and phi */
         const PT h = (PT)0.5, one = (PT)1;
         if (active) {
             for (int slot = 0; slot < 2; slot++) {
@@ -429,8 +422,8 @@ fused_pipe_lp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, PipeSched sch, int *errfla
                 const PT pR = E ? (PT)s.phiE[rc] : row[x + 1];
                 const PT a0 = h * (one + pL), a1 = h * (one + pM), a2 = h * (one + pR);
                 const PT b0 = h * (one - pL), b1 = h * (one - pM), b2 = h * (one - pR);
-                ap[slot][0] = a0 * a0; ap[slot][1] = a1 * a1; ap[slot][2] = a2 * a2;
-                am[slot][0] = b0 * b0; am[slot][1] = b1 * b1; am[slot][2] = b2 * b2;
+                ap[slot] = a0 * a0 + a1 * a1 + a2 * a2;
+                am[slot] = b0 * b0 + b1 * b1 + b2 * b2;
                 pc[slot] = pM;
             }
         }
@@ -458,8 +451,8 @@ fused_pipe_lp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, PipeSched sch, int *errfla
                     const PT pR = E ? (PT)s.phiE[rc] : sphi[Gm::ALP + tid + 1];
                     const PT a0 = h * (one + pL), a1 = h * (one + pM), a2 = h * (one + pR);
                     const PT b0 = h * (one - pL), b1 = h * (one - pM), b2 = h * (one - pR);
-                    ap[2][0] = a0 * a0; ap[2][1] = a1 * a1; ap[2][2] = a2 * a2;
-                    am[2][0] = b0 * b0; am[2][1] = b1 * b1; am[2][2] = b2 * b2;
+                    ap[2] = a0 * a0 + a1 * a1 + a2 * a2;
+                    am[2] = b0 * b0 + b1 * b1 + b2 * b2;
                     pc[2] = pM;
                 }
                 AT f[9], g[9];
@@ -502,12 +495,9 @@ fused_pipe_lp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, PipeSched sch, int *errfla
                     g[6] = (AT)C::lds(sg + 6 * Gm::RW + col + 1, isg);
                     g[7] = (AT)C::lds(sg + 7 * Gm::RW + col + 1, isg);
                 }
-                node_lp<S, PT, AT, TANH, MOM>(s, c, x, y, cc, E, f, g, ap, am, pc);
-#pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    ap[0][k] = ap[1][k]; ap[1][k] = ap[2][k];
-                    am[0][k] = am[1][k]; am[1][k] = am[2][k];
-                }
+                node_lp<S, PT, AT, TANH, MOM>(s, c, x, y, cc, E, f, g, (ap[0] + ap[1]) + ap[2], (am[0] + am[1]) + am[2], pc[1]);
+                ap[0] = ap[1]; ap[1] = ap[2];
+                am[0] = am[1]; am[1] = am[2];
                 pc[0] = pc[1]; pc[1] = pc[2];
             }
             __syncwarp();
