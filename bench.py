@@ -338,6 +338,27 @@ def main():
         forms[form] = {"glups": g, "hbm_gbs": g * b, "frac_of_measured_hbm": g * b / hbm,
                        "bytes_per_node": b, "speedup_vs_headline": g / (value / world)}
 
+    # the precision-form workload (4096^2, Ra 1e7): FP32 storage against FP64
+    precision_cfg = None
+    if world == 1 and "f32" in args.forms.split(",") and args.precision == "f64":
+        pwl = "cavity4096_ra1e7"
+        pparams = inputs.workload_params(**inputs.WORKLOADS[pwl])
+        pn = pparams["Nx"] * pparams["Ny"]
+        rates = {}
+        for prec in ("f64", "f32"):
+            s = Solver(pparams, precision=prec, device=local)
+            s.initialization()
+            s.step(args.warmup)
+            s.sync()
+            k = 400
+            pms = time_steps(s, k, torch)
+            s.close()
+            rates[prec] = pn * k / (pms / 1e3) / 1e9
+        precision_cfg = {"workload": pwl, "steps": 400, "f64_glups": rates["f64"], "f32_glups": rates["f32"],
+                         "f32_over_f64": rates["f32"] / rates["f64"],
+                         "f32_hbm_gbs": rates["f32"] * BYTES_PER_NODE["f32"],
+                         "f32_frac_of_measured_hbm": rates["f32"] * BYTES_PER_NODE["f32"] / hbm}
+
     adjoint = None
     if rank == 0 and world == 1 and not args.no_adjoint:
         adjoint = adjoint_cost(torch)
@@ -376,6 +397,7 @@ def main():
                          "frac": achieved / hbm, "traffic": traffic, "peak_kind": hbm_kind,
                          "bytes_per_node": bpn},
             "forms": forms,
+            "precision_config": precision_cfg,
             "adjoint": adjoint,
             "clocks": clocks,
             "e2e": e2e,

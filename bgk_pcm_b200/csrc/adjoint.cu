@@ -454,8 +454,21 @@ __device__ __forceinline__ double row3(const double *v, int i, bool hasL, bool h
     return (hasL ? v[i - 1] : 0.0) + v[i] + (hasR ? v[i + 1] : 0.0);
 }
 
-template <int ADJ_D, int ADJ_CTAS>
-__global__ void __launch_bounds__(PIPE_THREADS, ADJ_CTAS)
+/* Register split (WSPLIT): the CTA is two warpgroups, the four consumer
+ * warps and a producer warpgroup whose warp 4 lane 0 issues the copies.  It
+ * is launched with ADJ_LAUNCH_REGS registers per thread; the producer
+ * warpgroup gives all but ADJ_PROD_REGS back (setmaxnreg.dec) and the
+ * consumers take them (setmaxnreg.inc to ADJ_CONS_REGS), so the node VJP
+ * runs without spills at two CTAs per SM.  The two shares add up to the
+ * launch allocation exactly: ADJ_CONS_REGS + ADJ_PROD_REGS =
+ * 2 * ADJ_LAUNCH_REGS; the host checks the kernel's register count before
+ * it selects this variant. */
+constexpr int ADJ_LAUNCH_REGS = 128, ADJ_PROD_REGS = 40, ADJ_CONS_REGS = 216;
+static_assert(ADJ_CONS_REGS + ADJ_PROD_REGS == 2 * ADJ_LAUNCH_REGS, "register split must match the launch");
+static_assert(ADJ_CONS_REGS % 8 == 0 && ADJ_PROD_REGS % 8 == 0 && ADJ_PROD_REGS >= 24, "setmaxnreg granularity");
+
+template <int ADJ_D, int ADJ_CTAS, bool WSPLIT = false>
+__global__ void __launch_bounds__(WSPLIT ? 256 : PIPE_THREADS, ADJ_CTAS)
 adj_pipe_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
 {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -472,8 +485,9 @@ adj_pipe_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
         mbar_fence_init();
     }
     __syncthreads();
-    if (warp == PIPE_CWARPS) {
-        if (lane != 0) return;
+    if (warp >= PIPE_CWARPS) {
+        if constexpr (WSPLIT) asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(ADJ_PROD_REGS));
+        if (warp != PIPE_CWARPS || lane != 0) return;
         PipeIter it;
         long long r = 0;
         bool ok = it.start(sch, Ny);
@@ -493,6 +507,7 @@ adj_pipe_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
         return;
     }
 
+    if constexpr (WSPLIT) asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(ADJ_CONS_REGS));
     const long long pl = s.plane;
     const int P = s.P;
     const double *__restrict__ PIN = s.pin;
@@ -828,10 +843,22 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
     dim3 blk(AB_X, AB_Y), grd((c->Nx + AB_X - 1) / AB_X, (Ny + AB_Y - 1) / AB_Y);
     int pgrid = 0, partials = 0;
     PipeSched psch{};
-    /* pipeline depth and CTAs per SM of the reverse step (BGK_ADJ_PIPE=1:
-     * one stage, three CTAs per SM) */
-    int adj_d = 2, adj_ctas = 2;
-    if (const char *v = getenv("BGK_ADJ_PIPE")) if (atoi(v) == 1) { adj_d = 1; adj_ctas = 3; }
+    /* variant of the reverse step: 2 = two stages, two CTAs per SM and the
+     * producer/consumer register split (default, when the kernel's launch
+     * register count makes the split exact); 0 = the same without the
+     * split; 1 = one stage, three CTAs per SM (BGK_ADJ_PIPE selects) */
+    int adj_var = 2;
+    if (const char *v = getenv("BGK_ADJ_PIPE")) adj_var = atoi(v);
+    if (adj_var == 2) {
+        cudaFuncAttributes fa{};
+        if (cudaFuncGetAttributes(&fa, adj_pipe_kernel<2, 2, true>) != cudaSuccess ||
+            fa.numRegs != ADJ_LAUNCH_REGS) {
+            (void)cudaGetLastError();
+            adj_var = 0;
+        }
+    }
+    if (adj_var < 0 || adj_var > 2) adj_var = 2;
+    const int adj_d = adj_var == 1 ? 1 : 2, adj_ctas = adj_var == 1 ? 3 : 2;
     if (akind == 1) {
         psch = adj_sched(c, adj_ctas, PIPE_BX, &pgrid);
         partials = PIPE_CWARPS;
@@ -926,8 +953,10 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
         a.tanh_mode = c->opt.tanh_mode;
         if (akind == 1)
         {
-            if (adj_d == 1)
+            if (adj_var == 1)
                 adj_pipe_kernel<1, 3><<<pgrid, PIPE_THREADS, adj_smem(1), st>>>(a, c->c, psch, c->errflag);
+            else if (adj_var == 2)
+                adj_pipe_kernel<2, 2, true><<<pgrid, 256, adj_smem(2), st>>>(a, c->c, psch, c->errflag);
             else
                 adj_pipe_kernel<2, 2><<<pgrid, PIPE_THREADS, adj_smem(2), st>>>(a, c->c, psch, c->errflag);
         }
@@ -939,8 +968,9 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
 
     if (akind == 1) {
         static std::atomic<unsigned long long> done{0};
-        static std::atomic<unsigned long long> done1{0};
-        if (adj_d == 1) ACK(pipe_configure(adj_pipe_kernel<1, 3>, adj_smem(1), c->dev, done1));
+        static std::atomic<unsigned long long> done1{0}, done2{0};
+        if (adj_var == 1) ACK(pipe_configure(adj_pipe_kernel<1, 3>, adj_smem(1), c->dev, done1));
+        else if (adj_var == 2) ACK(pipe_configure(adj_pipe_kernel<2, 2, true>, adj_smem(2), c->dev, done2));
         else ACK(pipe_configure(adj_pipe_kernel<2, 2>, adj_smem(2), c->dev, done));
     }
     ACK(cudaMemcpyAsync(dpi, spec->probe_i, spec->nprobes * sizeof(int), cudaMemcpyHostToDevice, st));

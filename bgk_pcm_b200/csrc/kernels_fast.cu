@@ -644,11 +644,12 @@ cudaError_t launch_lowp_t(bgk_ctx *c, bool moments)
     const int H = strip_height(c);
     dim3 grd((c->Nx + FUSED_BX - 1) / FUSED_BX, (c->Ny + H - 1) / H);
     if (c->tune_pipe) {
-        /* stages of ~11 KB (FP32) / ~6 KB (FP16).  Measured on B200 at 2048^2
-         * and 4096^2: 4 stages with 3 CTAs per SM is best for both forms
-         * (5 CTAs per SM lose ~20 %). */
+        /* stages of ~10 KB (FP32) / ~5 KB (FP16).  Measured on B200 at 2048^2
+         * and 4096^2 (sweep of 3..6 stages x 3..5 CTAs per SM): 4 stages
+         * with 4 CTAs per SM is best for both forms at 4096^2 and within 3 %
+         * of the best at 2048^2. */
         const int D = c->tune_D > 0 ? c->tune_D : 4;
-        const int ctas = c->tune_ctas > 0 ? c->tune_ctas : 3;
+        const int ctas = c->tune_ctas > 0 ? c->tune_ctas : 4;
         if (D <= 3) return pipe_lp_dispatch<S, PT, AT, 3>(c, s, lp, moments, ctas);
         if (D >= 6) return pipe_lp_dispatch<S, PT, AT, 6>(c, s, lp, moments, ctas);
         return pipe_lp_dispatch<S, PT, AT, 4>(c, s, lp, moments, ctas);
