@@ -485,6 +485,8 @@ adj_pipe_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
         mbar_fence_init();
     }
     __syncthreads();
+    pdl_allow_next();
+    pdl_wait();
     if (warp >= PIPE_CWARPS) {
         if constexpr (WSPLIT) asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(ADJ_PROD_REGS));
         if (warp != PIPE_CWARPS || lane != 0) return;
@@ -953,12 +955,14 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
         a.tanh_mode = c->opt.tanh_mode;
         if (akind == 1)
         {
+            cudaError_t e;
             if (adj_var == 1)
-                adj_pipe_kernel<1, 3><<<pgrid, PIPE_THREADS, adj_smem(1), st>>>(a, c->c, psch, c->errflag);
+                e = pdl_launch(adj_pipe_kernel<1, 3>, pgrid, PIPE_THREADS, adj_smem(1), st, a, c->c, psch, c->errflag);
             else if (adj_var == 2)
-                adj_pipe_kernel<2, 2, true><<<pgrid, 256, adj_smem(2), st>>>(a, c->c, psch, c->errflag);
+                e = pdl_launch(adj_pipe_kernel<2, 2, true>, pgrid, 256, adj_smem(2), st, a, c->c, psch, c->errflag);
             else
-                adj_pipe_kernel<2, 2><<<pgrid, PIPE_THREADS, adj_smem(2), st>>>(a, c->c, psch, c->errflag);
+                e = pdl_launch(adj_pipe_kernel<2, 2>, pgrid, PIPE_THREADS, adj_smem(2), st, a, c->c, psch, c->errflag);
+            if (e != cudaSuccess) return e;
         }
         else
             adj_step_kernel<<<grd, blk, 0, st>>>(a, c->c);

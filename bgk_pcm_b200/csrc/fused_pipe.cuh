@@ -88,6 +88,8 @@ fused_pipe_f64_kernel(StepPtrs<double> s, Consts c, const double *__restrict__ c
         mbar_fence_init();
     }
     __syncthreads();
+    pdl_allow_next();
+    pdl_wait();
 
     if (warp == PIPE_CWARPS) {
         /* ---------------- producer ---------------- */
@@ -234,8 +236,8 @@ inline cudaError_t pipe_f64_launch(const bgk_ctx *c, const StepPtrs<double> &s, 
     if (e != cudaSuccess) return e;
     int grid;
     const PipeSched sch = pipe_sched(c, ctas, 4, &grid);
-    fused_pipe_f64_kernel<D, T, M, R><<<grid, PIPE_THREADS, smem, c->stream>>>(s, c->c, c->corner, sch, c->errflag);
-    return cudaGetLastError();
+    return pdl_launch(fused_pipe_f64_kernel<D, T, M, R>, grid, PIPE_THREADS, smem, c->stream, s, c->c,
+                      (const double *)c->corner, sch, c->errflag);
 }
 
 template <int D>

@@ -378,6 +378,8 @@ fused_pipe_lp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, PipeSched sch, int *errfla
         mbar_fence_init();
     }
     __syncthreads();
+    pdl_allow_next();
+    pdl_wait();
     if (warp == PIPE_CWARPS) {
         if (lane != 0) return;
         PipeIter it;
@@ -519,8 +521,8 @@ cudaError_t pipe_lp_launch(bgk_ctx *c, const LpPtrs<S, PT> &s, const ConstsLP<AT
     if (e != cudaSuccess) return e;
     int grid;
     const PipeSched sch = pipe_sched(c, ctas, 8, &grid);
-    fused_pipe_lp_kernel<S, PT, AT, D, T, M><<<grid, PIPE_THREADS, smem, c->stream>>>(s, lp, sch, c->errflag);
-    return cudaGetLastError();
+    return pdl_launch(fused_pipe_lp_kernel<S, PT, AT, D, T, M>, grid, PIPE_THREADS, smem, c->stream, s, lp, sch,
+                      c->errflag);
 }
 
 template <typename S, typename PT, typename AT, int D>

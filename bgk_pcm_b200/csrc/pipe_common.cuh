@@ -136,4 +136,32 @@ inline cudaError_t pipe_configure(K kernel, size_t smem, int dev, std::atomic<un
     return e;
 }
 
+/* Programmatic dependent launch.  A pipeline kernel is launched with
+ * programmatic stream serialization: its CTAs may be scheduled while the
+ * previous kernel on the stream drains, set up their shared memory and
+ * mbarriers, and then wait (griddepcontrol.wait) until that kernel has
+ * completed and its writes are visible.  Nothing reads or writes global
+ * memory before the wait.  Each CTA also allows the next kernel to be
+ * scheduled early (griddepcontrol.launch_dependents), which takes effect
+ * once every CTA of this grid is running or done. */
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_allow_next() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t pdl_launch(void (*kernel)(KArgs...), int grid, int block, size_t smem, cudaStream_t st,
+                              Args &&...args)
+{
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 #endif
