@@ -378,7 +378,9 @@ fused_pipe_lp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, PipeSched sch, int *errfla
         mbar_fence_init();
     }
     __syncthreads();
-    pdl_allow_next();
+    /* the next grid is allowed in only as this CTA finishes: with four CTAs
+     * of this kernel per SM there is room for a fifth, and an early
+     * dependent CTA there would wait on the same SM as the running ones */
     pdl_wait();
     if (warp == PIPE_CWARPS) {
         if (lane != 0) return;
@@ -398,6 +400,7 @@ fused_pipe_lp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, PipeSched sch, int *errfla
         }
         for (long long q = (r > D ? r - D : 0); q < r; q++)
             if (!mbar_wait(&full[q % D], (uint32_t)((q / D) & 1))) atomicExch(errflag, 2);
+        pdl_allow_next();
         return;
     }
     const long long pl = s.plane;
@@ -509,6 +512,7 @@ fused_pipe_lp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, PipeSched sch, int *errfla
         } while (ok && it.t == tile);
         if (failed) break;
     }
+    pdl_allow_next();
 }
 
 template <typename S, typename PT, typename AT, int D, int T, bool M>
