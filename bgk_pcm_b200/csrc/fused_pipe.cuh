@@ -236,8 +236,14 @@ inline cudaError_t pipe_f64_launch(const bgk_ctx *c, const StepPtrs<double> &s, 
     if (e != cudaSuccess) return e;
     int grid;
     const PipeSched sch = pipe_sched(c, ctas, 4, &grid);
-    return pdl_launch(fused_pipe_f64_kernel<D, T, M, R>, grid, PIPE_THREADS, smem, c->stream, s, c->c,
-                      (const double *)c->corner, sch, c->errflag);
+    /* programmatic dependent launch on grids of up to 2^21 nodes, whose
+     * steps are short enough (tens of microseconds) for the launch gap to
+     * matter: +9 % at 512^2; on larger grids it measured ~1 % slower */
+    if ((long long)c->Nx * c->Ny <= (1LL << 21))
+        return pdl_launch(fused_pipe_f64_kernel<D, T, M, R>, grid, PIPE_THREADS, smem, c->stream, s, c->c,
+                          (const double *)c->corner, sch, c->errflag);
+    fused_pipe_f64_kernel<D, T, M, R><<<grid, PIPE_THREADS, smem, c->stream>>>(s, c->c, c->corner, sch, c->errflag);
+    return cudaGetLastError();
 }
 
 template <int D>

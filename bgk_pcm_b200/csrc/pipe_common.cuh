@@ -136,14 +136,16 @@ inline cudaError_t pipe_configure(K kernel, size_t smem, int dev, std::atomic<un
     return e;
 }
 
-/* Programmatic dependent launch.  A pipeline kernel is launched with
+/* Programmatic dependent launch.  Where it pays (the FP64 step on small
+ * grids, the adjoint's reverse step) a pipeline kernel is launched with
  * programmatic stream serialization: its CTAs may be scheduled while the
  * previous kernel on the stream drains, set up their shared memory and
  * mbarriers, and then wait (griddepcontrol.wait) until that kernel has
  * completed and its writes are visible.  Nothing reads or writes global
- * memory before the wait.  Each CTA also allows the next kernel to be
- * scheduled early (griddepcontrol.launch_dependents), which takes effect
- * once every CTA of this grid is running or done. */
+ * memory before the wait.  A CTA allows the next kernel to be scheduled
+ * (griddepcontrol.launch_dependents), which takes effect once every CTA of
+ * this grid has done so or exited.  Under a plain launch both instructions
+ * are no-ops. */
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_allow_next() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
