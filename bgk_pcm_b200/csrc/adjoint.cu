@@ -1010,12 +1010,13 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
         for (int sgi = nsnap - 1; sgi >= 0; sgi--) {
             const int n0 = sgi * K;
             const int n1 = (n0 + K < N) ? n0 + K : N;
-            /* states S(n0) .. S(n1-1) into seg[0 .. n1-n0-1] */
-            ACK(cudaMemcpyAsync(seg, snaps + (size_t)sgi * state_elems,
-                                (state_elems - 2 * state_guard) * sizeof(double), cudaMemcpyDeviceToDevice, st));
-            for (int n = n0 + 1; n < n1; n++)
-                ACK(fwd(seg + (size_t)(n - 1 - n0) * state_elems, seg + (size_t)(n - n0) * state_elems));
-            for (int n = n1; n > n0; n--) ACK(rstep(seg + (size_t)(n - 1 - n0) * state_elems));
+            /* S(n0) is the snapshot itself; S(n0+1) .. S(n1-1) are recomputed
+             * into seg[1 .. n1-n0-1] */
+            auto state = [&](int n) {
+                return n == n0 ? snaps + (size_t)sgi * state_elems : seg + (size_t)(n - n0) * state_elems;
+            };
+            for (int n = n0 + 1; n < n1; n++) ACK(fwd(state(n - 1), state(n)));
+            for (int n = n1; n > n0; n--) ACK(rstep(state(n - 1)));
         }
     } else {
         double *work[3] = {seg, seg + state_elems, seg + 2 * state_elems};
