@@ -109,16 +109,18 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_oracle_rate(params, budget_s: float = 15.0, max_steps: int = 400, threads: int = 0):
+def cpu_oracle_rate(params, budget_s: float = 15.0, max_steps: int = 400, threads: int = 0, warmup: int = 2):
     """GLUPS of the CPU oracle on whole steps of `params`, with `threads`
-    OpenMP threads (0: all host threads; 1: the serial STEP_7 restatement)."""
+    OpenMP threads (0: all host threads; 1: the serial STEP_7 restatement).
+    `warmup` untimed steps (at least 2) also size the timed sample."""
     from oracle import pyoracle
     threads = threads or os.cpu_count() or 1
     o = pyoracle.Oracle(params, threads=threads)
     o.initialization()
+    w = max(2, warmup)
     t0 = time.perf_counter()
-    o.step(2)
-    dt = (time.perf_counter() - t0) / 2
+    o.step(w)
+    dt = (time.perf_counter() - t0) / w
     n = int(max(2, min(max_steps, budget_s / max(dt, 1e-9))))
     t0 = time.perf_counter()
     o.step(n)
@@ -231,10 +233,12 @@ def run_reference(args, params, wl):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    glups, n, threads = cpu_oracle_rate(params, budget_s=min(60.0, 5.0 + 0.5 * args.steps), max_steps=args.steps)
+    w = max(2, args.warmup)
+    glups, n, threads = cpu_oracle_rate(params, budget_s=min(60.0, 5.0 + 0.5 * args.steps), max_steps=args.steps,
+                                        warmup=w)
     line = {
         "impl": "reference", "metric": METRIC, "value": glups, "unit": "GLUPS", "n_gpus": args.gpus,
-        "steps": n, "warmup": 0, "ms_per_step": params["Nx"] * params["Ny"] / glups / 1e6,
+        "steps": n, "warmup": w, "ms_per_step": params["Nx"] * params["Ny"] / glups / 1e6,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (the reference's initial condition on the generated input.dat)",
         "config": {"workload": args.workload, "Nx": params["Nx"], "Ny": params["Ny"], "Ra": wl["Ra"],
