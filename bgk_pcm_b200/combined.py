@@ -158,9 +158,10 @@ def main(argv=None):
     ap.add_argument("--nprobes", type=int, default=64)
     ap.add_argument("--checkpoint-every", type=int, default=0)
     ap.add_argument("--precision", default="f32")
+    ap.add_argument("--h", default="1e-6,1e-4", help="finite-difference steps (comma list)")
     a = ap.parse_args(argv)
     r = run(a.nx, a.ny, a.ra, a.ste, a.steps, a.adjoint_steps, a.ndir, a.nprobes,
-            checkpoint_every=a.checkpoint_every, precision=a.precision)
+            h=tuple(float(x) for x in a.h.split(",")), checkpoint_every=a.checkpoint_every, precision=a.precision)
     print(json.dumps(r), flush=True)
 
 
