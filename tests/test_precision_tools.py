@@ -29,3 +29,17 @@ def test_errors_normalisation():
     assert abs(e["T_max"] - 0.01) < 1e-12 and abs(e["phi_max"] - 0.01) < 1e-12
     assert e["u_max"] == 0.0
     assert e["front_dx_max_cells"] == 0.0
+
+
+def test_front_probes_sit_behind_the_front():
+    from bgk_pcm_b200.combined import front_probes
+    ny, nx = 6, 10
+    phi = -np.ones((ny + 2, nx + 2))
+    fronts = [2, 3, 4, 5, 6, 7]          # last liquid column (1-based) of each interior row
+    for j, f in enumerate(fronts, start=1):
+        phi[j, 1:f + 1] = 1.0
+    pi, pj = front_probes(phi, 4, np.random.default_rng(0))
+    assert len(pi) == 4
+    for i, j in zip(pi, pj):
+        assert i == fronts[j - 1] + 1          # the first solid cell of its row
+        assert phi[j, i] < 0 and phi[j, i - 1] >= 0
