@@ -54,6 +54,26 @@ def test_fused_bit_exact(oracle_mod, lib, Nx, Ny):
         assert_fused_equal(o, s, f"after {done} steps")
 
 
+def test_fused_bit_exact_large_grid(oracle_mod, lib):
+    """Above 2^21 nodes the FP64 pipeline kernel is launched plainly (small
+    grids use programmatic dependent launch): same bits."""
+    o, s = make_pair(oracle_mod, lib, 1536, 1400)
+    o.step(3)
+    s.step(3)
+    assert_fused_equal(o, s, "after 3 steps")
+
+
+@pytest.mark.parametrize("Nx,Ny", [(16, 12), (130, 3), (64, 48)])
+def test_register_pull_kernel_bit_exact(oracle_mod, lib, monkeypatch, Nx, Ny):
+    """The register-pull kernel (BGK_PIPE=0, read at bgk_create)."""
+    monkeypatch.setenv("BGK_PIPE", "0")
+    o, s = make_pair(oracle_mod, lib, Nx, Ny)
+    for n in (1, 9):
+        o.step(n)
+        s.step(n)
+        assert_fused_equal(o, s, f"after {o.it} steps")
+
+
 @pytest.mark.parametrize("Nx,Ny", [(16, 12), (13, 7), (1, 5), (6, 1)])
 def test_staged_bit_exact_every_stage(oracle_mod, lib, Nx, Ny):
     """Each staged entry point equals the reference subroutine on all 46
