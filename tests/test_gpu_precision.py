@@ -89,3 +89,15 @@ def test_lowp_staged_unsupported(lib):
     s.initialization()
     with pytest.raises(BGKError, match="UNSUPPORTED"):
         s.BC_f()
+
+
+@pytest.mark.parametrize("precision", ["f32", "f16"])
+def test_register_pull_and_pipeline_agree(lib, monkeypatch, precision):
+    """The two reduced-precision kernels share the node arithmetic, so the
+    register-pull kernel (BGK_PIPE=0) and the pipeline give the same bits."""
+    p = small_params(130, 37)
+    a = run(precision, p, 25)
+    monkeypatch.setenv("BGK_PIPE", "0")
+    b = run(precision, p, 25)
+    for n in a:
+        np.testing.assert_array_equal(a[n], b[n], err_msg=n)
