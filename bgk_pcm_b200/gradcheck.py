@@ -121,7 +121,7 @@ def adjoint_autograd(p, tin, steps, pi, pj, target, checkpoint_every=45):
     tau = torch.tensor(float(p["tau_g"]), dtype=torch.float64, requires_grad=True)
     loss = fn.apply(t, tau, p, steps, pi, pj, target, checkpoint_every)
     loss.backward()
-    return float(loss), t.grad.numpy().copy(), float(tau.grad)
+    return float(loss.detach()), t.grad.numpy().copy(), float(tau.grad)
 
 
 def cost_ratio(p, tin, steps, pi, pj, target, checkpoint_every=45, repeats=3):
