@@ -21,7 +21,8 @@
  * d/dTin per row from the west nodes' pulled-g partials.
  *
  * Forward states come from snapshots every K steps; each K-step segment is
- * recomputed with the fused kernel before it is reversed.
+ * recomputed with the fused kernel before it is reversed, except the last
+ * one, whose states the forward pass writes into the segment buffer.
  */
 #include <atomic>
 #include <cmath>
@@ -123,7 +124,6 @@ __device__ __forceinline__ void node_vjp(const Consts &c, int tanh_mode, const d
     const double omp = 1.0 - phn;
     const double FX = -(u * omp * 0.5);
     const double FY = FY0 - v * omp * 0.5;
-    const double orho = c.omega_f * rho;
     const double iorho = irho * inv_of;   /* 1 / (omega_f rho) */
     const double uf = u + FX * iorho, vf = v + FY * iorho;
     /* non-equilibrium moments of g; the polynomials P_k(uf, vf) and their
@@ -397,10 +397,29 @@ constexpr int ADJ_SEG_BYTES = ADJ_RW * (int)sizeof(double);
 constexpr int ADJ_NSEG = 40;
 constexpr int ADJ_STAGE_BYTES = ADJ_NSEG * ADJ_SEG_BYTES;
 constexpr int ADJ_HEADER = 256;
+/* Wall tables: the values a west (x = 0) or east (x = Nx-1) node reads from
+ * global memory outside the staged rows, for every row of a tile (at most
+ * ADJ_BND_ROWS rows, the largest tile height adj_sched picks).  The warp
+ * that holds the wall node fills its table once per tile, one lane per row,
+ * so the loads of all rows are in flight together; the node then reads them
+ * from shared memory.  Without the tables the wall lane issued ~20 dependent
+ * global loads per row and the CTAs of the two wall bands set the kernel's
+ * duration.  Value v of row r is at table[v * ADJ_BND_ROWS + r]. */
+constexpr int ADJ_BND_ROWS = 64;
+constexpr int ADJ_BND_VALS = 10;
+enum : int { BW_PHI, BW_BB1, BW_BB8, BW_BB5, BW_GW0, BW_GW1, BW_GW2, BW_F5, BW_F8 };       /* west */
+enum : int { BE_PHI, BE_BB3, BE_BB7, BE_BB6, BE_LT, BE_G3, BE_G6, BE_G7, BE_F6, BE_F7 };  /* east */
+static_assert(BW_F8 < ADJ_BND_VALS && BE_F7 < ADJ_BND_VALS, "wall table width");
+constexpr int ADJ_BND_BYTES = 2 * ADJ_BND_VALS * ADJ_BND_ROWS * (int)sizeof(double);
 /* stages D and CTAs per SM: (2, 2) keeps a stage in flight while the
  * consumers work (168 registers); (1, 3) trades that for 50 % more warps
  * (128 registers) */
-__host__ __device__ constexpr size_t adj_smem(int D) { return (size_t)ADJ_HEADER + (size_t)D * ADJ_STAGE_BYTES; }
+__host__ __device__ constexpr size_t adj_smem(int D)
+{
+    return (size_t)ADJ_HEADER + (size_t)D * ADJ_STAGE_BYTES + (size_t)ADJ_BND_BYTES;
+}
+static_assert(2 * (adj_smem(2) + 1024) <= 228 * 1024, "two CTAs per SM");
+static_assert(3 * (adj_smem(1) + 1024) <= 228 * 1024, "three CTAs per SM");
 
 __host__ __device__ constexpr int opp_of(int k) { return k == 0 ? 0 : (k <= 4 ? (k + 1) % 4 + 1 : (k + 1) % 4 + 5); }
 static_assert(opp_of(1) == 3 && opp_of(2) == 4 && opp_of(3) == 1 && opp_of(4) == 2, "opposites");
@@ -448,6 +467,65 @@ __device__ __forceinline__ void adj_issue(const AdjPtrs &s, int Ny, int x0, int 
     adj_issue_t<ADJ_RW>(s, Ny, x0, y, stage, full);
 }
 
+/* Fill the wall tables for rows ty0 .. ty0 + nrows - 1 of a tile, lane r
+ * taking rows r, r + 32, ...: west node x = 0 into bw, east node x = Nx - 1
+ * into be, each value read or formed exactly as the row loop of
+ * adj_step_kernel does.  The west node's dL/dTin update, which needs only
+ * Pi(n+1), is made here as well (row y's entry is updated by this lane
+ * alone in the step). */
+__device__ __forceinline__ void adj_fill_walls(const AdjPtrs &s, const Consts &c, const double *__restrict__ PIN,
+                                               int ty0, int nrows, bool west, bool east, int lane, double *bw,
+                                               double *be)
+{
+    const long long pl = s.plane;
+    const int P = s.P, Nx = c.Nx, Ny = c.Ny;
+    for (int r = lane; r < nrows; r += 32) {
+        const int y = ty0 + r;
+        const bool S = (y == 0), N = (y == Ny - 1);
+        const int ym = S ? y : y - 1, yp = N ? y : y + 1;
+        const int rc = clamp_row(y + 1, Ny);
+        if (east) {
+            const int x = Nx - 1;
+            const long long cc = (long long)y * P + x;
+            double *t = be + r;
+            t[BE_PHI * ADJ_BND_ROWS] = s.phiE[rc];
+            t[BE_BB3 * ADJ_BND_ROWS] = PIN[3 * pl + cc];
+            t[BE_BB7 * ADJ_BND_ROWS] = PIN[7 * pl + cc];
+            t[BE_BB6 * ADJ_BND_ROWS] = PIN[6 * pl + cc];
+            /* T(Nx, y) is read by the east pulls of pops 3, 6 and 7 of the
+             * next step */
+            double lT = 0.0;
+            lT += PIN[(9 + 3) * pl + cc] * c.w[3] * s.pE[y];
+            double a6 = 0.0, a7 = 0.0;
+            if (y + 1 < Ny) a6 += PIN[(9 + 6) * pl + cc + P];
+            if (y == 0) a6 += PIN[(9 + 6) * pl + x];
+            if (y - 1 >= 0) a7 += PIN[(9 + 7) * pl + cc - P];
+            if (y == Ny - 1) a7 += PIN[(9 + 7) * pl + (long long)(Ny - 1) * P + x];
+            lT += a6 * c.w[6] * s.pE[Ny + y] + a7 * c.w[7] * s.pE[2 * Ny + y];
+            t[BE_LT * ADJ_BND_ROWS] = lT;
+            t[BE_G3 * ADJ_BND_ROWS] = c.w[3] * s.tcol[y] * s.pE[y];
+            t[BE_G6 * ADJ_BND_ROWS] = c.w[6] * s.tcol[ym] * s.pE[Ny + ym];
+            t[BE_G7 * ADJ_BND_ROWS] = c.w[7] * s.tcol[yp] * s.pE[2 * Ny + yp];
+            t[BE_F6 * ADJ_BND_ROWS] = S ? s.corner[0] : s.f[8 * pl + cc];
+            t[BE_F7 * ADJ_BND_ROWS] = N ? s.corner[1] : s.f[5 * pl + cc];
+        }
+        if (west) {
+            const long long cc = (long long)y * P;
+            double *t = bw + r;
+            t[BW_PHI * ADJ_BND_ROWS] = s.phiW[rc];
+            t[BW_BB1 * ADJ_BND_ROWS] = PIN[1 * pl + cc];
+            t[BW_BB8 * ADJ_BND_ROWS] = PIN[8 * pl + cc];
+            t[BW_BB5 * ADJ_BND_ROWS] = PIN[5 * pl + cc];
+            t[BW_GW0 * ADJ_BND_ROWS] = s.gW[y];
+            t[BW_GW1 * ADJ_BND_ROWS] = s.gW[Ny + ym];
+            t[BW_GW2 * ADJ_BND_ROWS] = s.gW[2 * Ny + yp];
+            t[BW_F5 * ADJ_BND_ROWS] = s.f[7 * pl + cc];
+            t[BW_F8 * ADJ_BND_ROWS] = s.f[6 * pl + cc];
+            s.gtin[y] += tin_partial(PIN, pl, P, Ny, s.dgW, y);
+        }
+    }
+}
+
 /* Sum of a Pi row over columns x-1..x+1 inside the domain. */
 __device__ __forceinline__ double row3(const double *v, int i, bool hasL, bool hasR)
 {
@@ -475,6 +553,7 @@ adj_pipe_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
     uint64_t *full = reinterpret_cast<uint64_t *>(smem);
     uint64_t *empty = full + ADJ_D;
     unsigned char *stages = smem + ADJ_HEADER;
+    double *bwall = reinterpret_cast<double *>(stages + (size_t)ADJ_D * ADJ_STAGE_BYTES);   /* wall tables */
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int Nx = c.Nx, Ny = c.Ny;
     if (tid == 0) {
@@ -543,6 +622,22 @@ adj_pipe_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
                 }
             }
         }
+        /* wall tables of this tile, filled by the warp that holds the west
+         * or east node (warp-private: only that warp's lanes touch them) */
+        const int ty0 = it.y;
+        const int eoff = Nx - 1 - it.x0;
+        const bool wwest = it.x0 == 0 && warp == 0;
+        const bool weast = eoff < PIPE_BX && warp == (eoff >> 5);
+        if (wwest || weast) {
+            int nrows = it.y1 - it.y;
+            if (nrows > ADJ_BND_ROWS) {         /* adj_sched never picks such H */
+                if (lane == 0) atomicExch(errflag, 14);
+                nrows = ADJ_BND_ROWS;
+            }
+            __syncwarp();
+            adj_fill_walls(s, c, PIN, ty0, nrows, wwest, weast, lane, bwall, bwall + ADJ_BND_VALS * ADJ_BND_ROWS);
+            __syncwarp();
+        }
         const int tile = it.t;
         bool failed = false;
         do {
@@ -559,13 +654,16 @@ adj_pipe_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
                 const bool S = (y == 0), N = (y == Ny - 1);
                 const long long cc = (long long)y * P + x;
                 const int col = tid + ADJ_AL;
+                /* this row's entries of the wall tables */
+                const int rl = (y - ty0) & (ADJ_BND_ROWS - 1);
+                auto wv = [&](int v) { return bwall[v * ADJ_BND_ROWS + rl]; };
+                auto ev = [&](int v) { return bwall[(ADJ_BND_VALS + v) * ADJ_BND_ROWS + rl]; };
                 /* new row y+1 of both windows */
                 {
-                    const int rc = clamp_row(y + 1, Ny);
                     const double *sph = stg + 39 * ADJ_RW;
-                    ph[2][0] = W ? s.phiW[rc] : sph[col - 1];
+                    ph[2][0] = W ? wv(BW_PHI) : sph[col - 1];
                     ph[2][1] = sph[col];
-                    ph[2][2] = E ? s.phiE[rc] : sph[col + 1];
+                    ph[2][2] = E ? ev(BE_PHI) : sph[col + 1];
                     if (y + 1 < Ny) {
                         rk[2] = row3(stg + 18 * ADJ_RW, col, hasL, hasR);
                         rm[2] = row3(stg + 19 * ADJ_RW, col, hasL, hasR);
@@ -594,7 +692,14 @@ adj_pipe_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
                              * pop 7 at (Nx,Ny)) */
                             const bool corner6 = (k == 8) && E && S;
                             const bool corner7 = (k == 5) && E && N;
-                            *wf = (corner6 || corner7) ? 0.0 : PIN[opp_of(k) * pl + cc];
+                            double v;
+                            if (cx_of(k) == -1 && W)
+                                v = wv(k == 3 ? BW_BB1 : (k == 6 ? BW_BB8 : BW_BB5));
+                            else if (cx_of(k) == 1 && E)
+                                v = ev(k == 1 ? BE_BB3 : (k == 5 ? BE_BB7 : BE_BB6));
+                            else
+                                v = PIN[opp_of(k) * pl + cc];
+                            *wf = (corner6 || corner7) ? 0.0 : v;
                         }
                         double a = 0.0;
                         if (xin) {
@@ -608,18 +713,9 @@ adj_pipe_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
                 const double skp = rk[0] + rk[1] + rk[2] + (S ? rk[1] : 0.0) + (N ? rk[1] : 0.0);
                 const double skm = rm[0] + rm[1] + rm[2] + (S ? rm[1] : 0.0) + (N ? rm[1] : 0.0);
                 const double d0 = stg[20 * ADJ_RW + col];
-                double lT = 0.0;
-                if (E) {
-                    lT += PIN[(9 + 3) * pl + cc] * c.w[3] * s.pE[y];
-                    double a6 = 0.0, a7 = 0.0;
-                    if (y + 1 < Ny) a6 += PIN[(9 + 6) * pl + cc + P];
-                    if (y == 0) a6 += PIN[(9 + 6) * pl + x];
-                    if (y - 1 >= 0) a7 += PIN[(9 + 7) * pl + cc - P];
-                    if (y == Ny - 1) a7 += PIN[(9 + 7) * pl + (long long)(Ny - 1) * P + x];
-                    lT += a6 * c.w[6] * s.pE[Ny + y] + a7 * c.w[7] * s.pE[2 * Ny + y];
-                }
-                /* dL/dTin from Pi(n+1), one thread per row */
-                if (W) s.gtin[y] += tin_partial(PIN, pl, P, Ny, s.dgW, y);
+                /* T(Nx, y) partial (east); the west node's dL/dTin update was
+                 * made when the wall table was filled */
+                const double lT = E ? ev(BE_LT) : 0.0;
 
                 /* 2. pulled inputs of step n from S(n-1), as the forward pipeline */
                 const double *sp = stg + 21 * ADJ_RW, *sg = stg + 30 * ADJ_RW;
@@ -637,28 +733,31 @@ adj_pipe_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
                 if (W || E || S || N) {
                     if (S) f[2] = F[4 * pl + cc];
                     if (N) f[4] = F[2 * pl + cc];
-                    if (W || S) f[5] = F[7 * pl + cc];
-                    if (E || S) f[6] = (E && S) ? s.corner[0] : F[8 * pl + cc];
-                    if (E || N) f[7] = (E && N) ? s.corner[1] : F[5 * pl + cc];
-                    if (W || N) f[8] = F[6 * pl + cc];
+                    if (W) f[5] = wv(BW_F5);
+                    else if (S) f[5] = F[7 * pl + cc];
+                    if (E) f[6] = ev(BE_F6);
+                    else if (S) f[6] = F[8 * pl + cc];
+                    if (E) f[7] = ev(BE_F7);
+                    else if (N) f[7] = F[5 * pl + cc];
+                    if (W) f[8] = wv(BW_F8);
+                    else if (N) f[8] = F[6 * pl + cc];
                 }
-                const int ym = S ? y : y - 1, yp = N ? y : y + 1;
                 g[0] = sg[0 * ADJ_RW + col];
                 g[2] = sg[2 * ADJ_RW + col];
                 g[4] = sg[4 * ADJ_RW + col];
                 if (W) {
-                    g[1] = s.gW[y];
-                    g[5] = s.gW[Ny + ym];
-                    g[8] = s.gW[2 * Ny + yp];
+                    g[1] = wv(BW_GW0);
+                    g[5] = wv(BW_GW1);
+                    g[8] = wv(BW_GW2);
                 } else {
                     g[1] = sg[1 * ADJ_RW + col - 1];
                     g[5] = sg[5 * ADJ_RW + col - 1];
                     g[8] = sg[8 * ADJ_RW + col - 1];
                 }
                 if (E) {
-                    g[3] = c.w[3] * s.tcol[y] * s.pE[y];
-                    g[6] = c.w[6] * s.tcol[ym] * s.pE[Ny + ym];
-                    g[7] = c.w[7] * s.tcol[yp] * s.pE[2 * Ny + yp];
+                    g[3] = ev(BE_G3);
+                    g[6] = ev(BE_G6);
+                    g[7] = ev(BE_G7);
                 } else {
                     g[3] = sg[3 * ADJ_RW + col + 1];
                     g[6] = sg[6 * ADJ_RW + col + 1];
@@ -718,14 +817,14 @@ PipeSched adj_sched(const bgk_ctx *c, int ctas_per_sm, int bx, int *grid)
     const long long slots = (long long)c->nsm * ctas_per_sm;
     long long best = -1;
     int bestH = 1;
-    for (int H = 1; H <= 64; H++) {
+    for (int H = 1; H <= ADJ_BND_ROWS; H++) {
         const long long tiles = (long long)sch.nbands * ((c->Ny + H - 1) / H);
         const long long waves = (tiles + slots - 1) / slots;
         const long long cost = waves * (H + 1);
         if (best < 0 || cost < best) { best = cost; bestH = H; }
         if (H >= c->Ny) break;
     }
-    if (c->tune_H > 0) bestH = c->tune_H;
+    if (c->tune_H > 0) bestH = c->tune_H < ADJ_BND_ROWS ? c->tune_H : ADJ_BND_ROWS;   /* wall tables */
     sch.H = bestH;
     sch.nstrips = (c->Ny + bestH - 1) / bestH;
     sch.ntiles = sch.nbands * sch.nstrips;
@@ -860,7 +959,7 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
         }
     }
     if (adj_var < 0 || adj_var > 2) adj_var = 2;
-    const int adj_d = adj_var == 1 ? 1 : 2, adj_ctas = adj_var == 1 ? 3 : 2;
+    const int adj_ctas = adj_var == 1 ? 3 : 2;
     if (akind == 1) {
         psch = adj_sched(c, adj_ctas, PIPE_BX, &pgrid);
         partials = PIPE_CWARPS;
@@ -935,6 +1034,15 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
             return e;
         return cudaMemcpyAsync(dst + 19 * pl, c->tcol[buf], Ny * sizeof(double), cudaMemcpyDeviceToDevice, st);
     };
+    auto copy_state_out = [&](int buf, const double *src) -> cudaError_t {
+        cudaError_t e;
+        if ((e = cudaMemcpyAsync(c->fbuf[buf], src, 9 * pl * sizeof(double), cudaMemcpyDeviceToDevice, st))) return e;
+        if ((e = cudaMemcpyAsync(c->gbuf[buf], src + 9 * pl, 9 * pl * sizeof(double), cudaMemcpyDeviceToDevice, st)))
+            return e;
+        if ((e = cudaMemcpyAsync(c->phibuf[buf], src + 18 * pl, pl * sizeof(double), cudaMemcpyDeviceToDevice, st)))
+            return e;
+        return cudaMemcpyAsync(c->tcol[buf], src + 19 * pl, Ny * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    };
     /* one fused forward step between two stored states */
     auto fwd = [&](const double *a, double *b) -> cudaError_t {
         return bgk::launch_fused_f64_ptrs(c, a, a + 9 * pl, a + 18 * pl, a + 19 * pl, b, b + 9 * pl, b + 18 * pl,
@@ -986,15 +1094,40 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
     /* forward pass on the context (snapshots every K steps in the sqrt(N)
      * scheme; S(0) only in the binomial one) */
     ACK(copy_state_in(snaps, c->cur));
+    bool last_in_seg = false;             /* the last segment's states are in seg */
     if (binomial) {
         rc = bgk_step(c, N);
         if (rc) { cleanup(); return rc; }
     } else {
         for (int n0 = 0; n0 < N; n0 += K) {
             const int len = (n0 + K < N) ? K : N - n0;
-            rc = (n0 + len < N) ? bgk_internal_advance(c, len) : bgk_step(c, len);
-            if (rc) { cleanup(); return rc; }
-            if (n0 + len < N) ACK(copy_state_in(snaps + (size_t)((n0 + len) / K) * state_elems, c->cur));
+            if (n0 + len < N) {
+                rc = bgk_internal_advance(c, len);
+                if (rc) { cleanup(); return rc; }
+                ACK(copy_state_in(snaps + (size_t)((n0 + len) / K) * state_elems, c->cur));
+            } else if (len >= 3) {
+                /* last segment: S(n0+1) .. S(N-2) go straight into the
+                 * segment buffer, so the reverse sweep need not recompute
+                 * them; S(N-2) is copied into the context, whose last two
+                 * steps run through bgk_step (moments and halos), and S(N-1)
+                 * is copied back from the context's other buffer */
+                rc = bgk_internal_prepare_fused(c);
+                if (rc) { cleanup(); return rc; }
+                const double *s0 = snaps + (size_t)(n0 / K) * state_elems;
+                for (int n = n0 + 1; n <= N - 2; n++)
+                    ACK(fwd(n - 1 == n0 ? s0 : seg + (size_t)(n - 1 - n0) * state_elems,
+                            seg + (size_t)(n - n0) * state_elems));
+                ACK(copy_state_out(c->cur, seg + (size_t)(N - 2 - n0) * state_elems));
+                c->it += len - 2;
+                c->pristine = false;
+                rc = bgk_step(c, 2);
+                if (rc) { cleanup(); return rc; }
+                ACK(copy_state_in(seg + (size_t)(N - 1 - n0) * state_elems, c->cur ^ 1));
+                last_in_seg = true;
+            } else {
+                rc = bgk_step(c, len);
+                if (rc) { cleanup(); return rc; }
+            }
         }
     }
     /* loss and seed */
@@ -1015,7 +1148,8 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
             auto state = [&](int n) {
                 return n == n0 ? snaps + (size_t)sgi * state_elems : seg + (size_t)(n - n0) * state_elems;
             };
-            for (int n = n0 + 1; n < n1; n++) ACK(fwd(state(n - 1), state(n)));
+            if (!(last_in_seg && sgi == nsnap - 1))
+                for (int n = n0 + 1; n < n1; n++) ACK(fwd(state(n - 1), state(n)));
             for (int n = n1; n > n0; n--) ACK(rstep(state(n - 1)));
         }
     } else {
