@@ -193,17 +193,32 @@ __device__ __forceinline__ double tanh_pt<double>(double x, int mode)
 
 /* One node of a reduced-precision step after its pulls (deviations in AT):
  * momentsPre, phase field (PT), latent heat (FP64), forces, collision,
- * stores, moments.  Shared by the register-pull and pipeline kernels. */
+ * stores, moments.  Shared by the register-pull and pipeline kernels.
+ *
+ * Conservation closure.  In exact arithmetic the collision leaves sum_k f_k
+ * and sum_k g_k unchanged (the latter after the latent heat).  Evaluated in
+ * FP32 it does not: the g equilibrium carries terms w_k T0 Q_k of ~30 K
+ * against an energy deviation of a few K, and in a steady flow the same
+ * rounding recurs at a node every step, so it acts as a spurious heat (and
+ * mass) source.  At 256^2 that source moved T by 1.7e-4 dT and the melt
+ * front by 0.002 cells after 20k steps.  So the rest populations are the
+ * residuals: f_0 = drho - sum_{k>0} f_k in AT, and g_0 = dT - sum_{k>0} g_k
+ * in FP64, with dT, the node's energy deviation, also summed and carried
+ * through the latent heat in FP64 (the energy bookkeeping of the
+ * liquid-fraction update).  The stored populations then carry the node's
+ * mass and energy up to the rounding of f_0 and g_0 themselves. */
 template <typename S, typename PT, typename AT, int TANH, bool MOM>
 __device__ __forceinline__ void node_lp(const LpPtrs<S, PT> &s, const ConstsLP<AT> &c, int x, int y, long long cc,
                                         bool E, AT *f, AT *g, PT kp, PT km, PT p0)
 {
     using C = Codec<S>;
     const long long pl = s.plane;
-    /* momentsPre (deviations) */
-    AT drho = 0, dT = 0;
+    /* momentsPre (deviations; the energy in FP64) */
+    AT drho = 0;
+    double dTd = 0.0;
 #pragma unroll
-    for (int k = 0; k < 9; k++) { drho += f[k]; dT += g[k]; }
+    for (int k = 0; k < 9; k++) { drho += f[k]; dTd += (double)g[k]; }
+    AT dT = (AT)dTd;
     const AT rho = c.rho0 + drho;
     const AT irho = (AT)1 / rho;
     AT u = irho * (f[1] - f[3] + f[5] - f[6] - f[7] + f[8]);
@@ -219,7 +234,8 @@ __device__ __forceinline__ void node_lp(const LpPtrs<S, PT> &s, const ConstsLP<A
     const AT phn = (AT)phn_p;
 
     /* forces: latent heat in FP64 */
-    dT = (AT)((double)dT - c.dts * ((double)phn_p - (double)p0) * 0.5);
+    dTd -= c.dts * ((double)phn_p - (double)p0) * 0.5;
+    dT = (AT)dTd;
     const AT T = c.T0 + dT;
     const AT omp = (AT)1 - phn;
     const AT forceY = rho * c.gb * T * ((AT)1 + (AT)0.5 * phn) - (AT)0.5 * v * omp;
@@ -235,12 +251,24 @@ __device__ __forceinline__ void node_lp(const LpPtrs<S, PT> &s, const ConstsLP<A
     for (int k = 0; k < 9; k++) eq[k] = c.w[k] * (c.rho0 * Q[k] + drho * ((AT)1 + Q[k]));
     eq[0] += c.wcorr * drho;
     reg_relax_lp(c, f, eq, c.cf, out);
+    {
+        AT r = drho;                        /* mass closure */
+#pragma unroll
+        for (int k = 1; k < 9; k++) r -= out[k];
+        out[0] = r;
+    }
 #pragma unroll
     for (int k = 0; k < 9; k++) { C::st(s.fout + k * pl + cc, (float)out[k], s.sf); f[k] = out[k]; }
 #pragma unroll
     for (int k = 0; k < 9; k++) eq[k] = c.w[k] * (c.T0 * Q[k] + dT * ((AT)1 + Q[k]));
     eq[0] += c.wcorr * dT;
     reg_relax_lp(c, g, eq, c.cg, out);
+    {
+        double r = dTd;                     /* energy closure */
+#pragma unroll
+        for (int k = 1; k < 9; k++) r -= (double)out[k];
+        out[0] = (AT)r;
+    }
 #pragma unroll
     for (int k = 0; k < 9; k++) C::st(s.gout + k * pl + cc, (float)out[k], s.sg);
     s.phout[cc] = phn_p;
