@@ -127,6 +127,11 @@ def load() -> ctypes.CDLL:
         "bgk_load": (ctypes.c_int, [P, ctypes.c_char_p]),
         "bgk_adjoint_run": (ctypes.c_int, [P, ctypes.POINTER(AdjointSpec), dp, dp, dp]),
         "bgk_field_sums_static": (ctypes.c_int, [P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P]),
+        "bgk_advance": (ctypes.c_int, [P, ctypes.c_int]),
+        "bgk_rows_bytes": (ctypes.c_int, [P, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
+        "bgk_rows_pack": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, P]),
+        "bgk_rows_unpack": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, P]),
+        "bgk_field_sums_rows": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, dp]),
     }
     for n in ("bgk_bc_f", "bgk_bc_g", "bgk_streaming", "bgk_moments_pre", "bgk_phase_field",
               "bgk_forces", "bgk_collision", "bgk_moments"):

@@ -153,7 +153,9 @@ cudaError_t launch_compact_to_staged(bgk_ctx *c);
 cudaError_t launch_staged_to_compact(bgk_ctx *c);
 cudaError_t launch_ref_to_compact(bgk_ctx *c, int field, const double *ref);
 cudaError_t launch_compact_to_ref(bgk_ctx *c, int field, double *ref, int which);
-cudaError_t launch_field_sums(bgk_ctx *c);   /* -> c->red[0..3] */
+cudaError_t launch_field_sums(bgk_ctx *c, int j0, int nrows);   /* -> c->red[0..3] */
+size_t rows_bytes(const bgk_ctx *c, int nrows);                 /* packed slab halo rows */
+cudaError_t launch_rows_copy(bgk_ctx *c, int j0, int nrows, void *buf, bool unpack);
 cudaError_t launch_fused_f64_ptrs(bgk_ctx *c, const double *fin, const double *gin, const double *phin,
                                   const double *tcin, double *fout, double *gout, double *phout, double *tcout);
 

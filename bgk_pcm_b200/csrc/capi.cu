@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cerrno>
 #include <cmath>
+#include <cstdint>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -646,12 +647,14 @@ int bgk_download_region(bgk_ctx *c, int field, int i0, int j0, int ni, int nj, d
     return BGK_OK;
 }
 
-int bgk_field_sums(bgk_ctx *c, double out[4])
+static int field_sums_range(bgk_ctx *c, int j0, int nrows, double out[4])
 {
     if (!c || !out) return fail(BGK_ERR_ARG, "null argument");
+    if (j0 < 0 || nrows < 1 || (long long)j0 + nrows > c->Ny)
+        return fail(BGK_ERR_ARG, "rows %d..%d outside 0..%d", j0, j0 + nrows - 1, c->Ny - 1);
     int rc = set_device(c);
     if (rc) return rc;
-    CK(bgk::launch_field_sums(c), "field sums");
+    CK(bgk::launch_field_sums(c, j0, nrows), "field sums");
     CK(cudaMemcpyAsync(c->pinned, c->red, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "sums copy");
     CK(cudaStreamSynchronize(c->stream), "field sums");
     for (int k = 0; k < 4; k++) out[k] = c->pinned[k];
@@ -659,6 +662,55 @@ int bgk_field_sums(bgk_ctx *c, double out[4])
         if (!std::isfinite(out[k])) return fail(BGK_ERR_NONFINITE, "field sum %d is not finite", k);
     return BGK_OK;
 }
+
+int bgk_field_sums(bgk_ctx *c, double out[4])
+{
+    if (!c) return fail(BGK_ERR_ARG, "null context");
+    return field_sums_range(c, 0, c->Ny, out);
+}
+
+int bgk_field_sums_rows(bgk_ctx *c, int j0, int nrows, double out[4]) { return field_sums_range(c, j0, nrows, out); }
+
+int bgk_advance(bgk_ctx *c, int nsteps)
+{
+    if (!c) return fail(BGK_ERR_ARG, "null context");
+    if (nsteps < 0) return fail(BGK_ERR_ARG, "nsteps < 0");
+    if (nsteps == 0) return BGK_OK;
+    return bgk_internal_advance(c, nsteps);
+}
+
+int bgk_rows_bytes(const bgk_ctx *c, int nrows, size_t *bytes)
+{
+    if (!c || !bytes) return fail(BGK_ERR_ARG, "null argument");
+    if (nrows < 1 || nrows > c->Ny) return fail(BGK_ERR_ARG, "nrows %d outside 1..%d", nrows, c->Ny);
+    *bytes = bgk::rows_bytes(c, nrows);
+    return BGK_OK;
+}
+
+static int rows_copy(bgk_ctx *c, int j0, int nrows, const void *buf, bool unpack)
+{
+    if (!c || !buf) return fail(BGK_ERR_ARG, "null argument");
+    if (j0 < 0 || nrows < 1 || (long long)j0 + nrows > c->Ny)
+        return fail(BGK_ERR_ARG, "rows %d..%d outside 0..%d", j0, j0 + nrows - 1, c->Ny - 1);
+    if ((uintptr_t)buf & 15u) return fail(BGK_ERR_ARG, "row buffer is not 16-byte aligned");
+    int rc = set_device(c);
+    if (rc) return rc;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, buf) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(BGK_ERR_ARG, "row buffer is not a CUDA pointer");
+    }
+    if (!(at.type == cudaMemoryTypeManaged || (at.type == cudaMemoryTypeDevice && at.device == c->dev)))
+        return fail(BGK_ERR_ARG, "row buffer is not device memory of the context's device");
+    if ((rc = ensure_fused(c))) return rc;
+    CK(bgk::launch_rows_copy(c, j0, nrows, const_cast<void *>(buf), unpack), unpack ? "rows unpack" : "rows pack");
+    if (unpack) c->pristine = false;
+    return BGK_OK;
+}
+
+int bgk_rows_pack(bgk_ctx *c, int j0, int nrows, void *buf) { return rows_copy(c, j0, nrows, buf, false); }
+
+int bgk_rows_unpack(bgk_ctx *c, int j0, int nrows, const void *buf) { return rows_copy(c, j0, nrows, buf, true); }
 
 int bgk_get_it(const bgk_ctx *c, int *it)
 {

@@ -508,14 +508,14 @@ __device__ __forceinline__ double warp_sum(double v)
  * interior in a fixed order, each block reduces with warp shuffles and
  * writes 4 partials; one block then adds the partials in index order. */
 __global__ void field_sums_kernel(Consts c, const double *rho, const double *T, const double *phi,
-                                  double *partial)
+                                  double *partial, int j0, int nrows)
 {
-    const int Nx = c.Nx, Ny = c.Ny, NX2 = Nx + 2;
-    const long long n = (long long)Nx * Ny;
+    const int Nx = c.Nx, NX2 = Nx + 2;
+    const long long n = (long long)Nx * nrows;
     double a = 0.0, b = 0.0, p = 0.0, k = 0.0;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(t % Nx) + 1, j = (int)(t / Nx) + 1;
+        const int i = (int)(t % Nx) + 1, j = (int)(t / Nx) + 1 + j0;
         const size_t q = SQ(i, j);
         a += rho[q];
         b += T[q];
@@ -737,12 +737,97 @@ cudaError_t launch_compact_to_ref(bgk_ctx *c, int field, double *ref, int which)
     return cudaGetLastError();
 }
 
-/* Results land in c->red[0..3]. */
-cudaError_t launch_field_sums(bgk_ctx *c)
+/* Interior rows j0 .. j0+nrows-1 (0-based); results land in c->red[0..3]. */
+cudaError_t launch_field_sums(bgk_ctx *c, int j0, int nrows)
 {
-    field_sums_kernel<<<SUM_BLOCKS, SUM_THREADS, 0, c->stream>>>(c->c, c->mrho, c->mT, c->mphi, c->red);
+    field_sums_kernel<<<SUM_BLOCKS, SUM_THREADS, 0, c->stream>>>(c->c, c->mrho, c->mT, c->mphi, c->red, j0,
+                                                                  nrows);
     field_sums_final<<<1, 32, 0, c->stream>>>(c->red);
     return cudaGetLastError();
+}
+
+/* ------------------------------------------------------- slab halo rows */
+
+/* Packed rows: 20 sections (f_0..f_8, g_0..g_8 of TE, phi of TP, the east
+ * T column of double), each nrows x Nx elements (the T column nrows) and
+ * padded to 16 bytes.  blockIdx.y is the section; a grid-stride loop over
+ * its elements.  UNPACK copies the other way. */
+__host__ __device__ inline size_t rows_section_bytes(long long elems, int esz)
+{
+    return ((size_t)elems * (size_t)esz + 15) / 16 * 16;
+}
+
+template <typename TE, typename TP, bool UNPACK>
+__global__ void rows_copy_kernel(TE *f, TE *g, TP *phi, double *tcol, long long pl, int P, int Nx, int j0,
+                                 int nrows, unsigned char *buf)
+{
+    const int sec = blockIdx.y;
+    const long long n = (long long)Nx * nrows;
+    const size_t sec_pop = rows_section_bytes(n, (int)sizeof(TE));
+    if (sec < 19) {
+        size_t off;
+        if (sec < 18) off = (size_t)sec * sec_pop;
+        else off = 18 * sec_pop;
+        for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+             t += (long long)gridDim.x * blockDim.x) {
+            const long long r = t / Nx, x = t % Nx;
+            const long long q = (long long)(j0 + r) * P + x;
+            if (sec < 18) {
+                TE *plane = (sec < 9 ? f + (long long)sec * pl : g + (long long)(sec - 9) * pl);
+                TE *b = reinterpret_cast<TE *>(buf + off);
+                if (UNPACK) plane[q] = b[t];
+                else b[t] = plane[q];
+            } else {
+                TP *b = reinterpret_cast<TP *>(buf + off);
+                if (UNPACK) phi[q] = b[t];
+                else b[t] = phi[q];
+            }
+        }
+    } else {
+        double *b = reinterpret_cast<double *>(buf + 18 * sec_pop + rows_section_bytes(n, (int)sizeof(TP)));
+        for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nrows;
+             t += (long long)gridDim.x * blockDim.x) {
+            if (UNPACK) tcol[j0 + t] = b[t];
+            else b[t] = tcol[j0 + t];
+        }
+    }
+}
+
+size_t rows_bytes(const bgk_ctx *c, int nrows)
+{
+    const long long n = (long long)c->Nx * nrows;
+    return 18 * rows_section_bytes(n, c->esz) + rows_section_bytes(n, c->phisz) + rows_section_bytes(nrows, 8);
+}
+
+template <typename TE, typename TP>
+static cudaError_t rows_copy_t(bgk_ctx *c, int j0, int nrows, unsigned char *buf, bool unpack)
+{
+    const int cur = c->cur;
+    TE *f = static_cast<TE *>(c->fbuf[cur]);
+    TE *g = static_cast<TE *>(c->gbuf[cur]);
+    TP *phi = static_cast<TP *>(c->phibuf[cur]);
+    const long long n = (long long)c->Nx * nrows;
+    long long bx = (n + 255) / 256;
+    if (bx > 1184) bx = 1184;
+    const dim3 grd((unsigned)bx, 20);
+    if (unpack)
+        rows_copy_kernel<TE, TP, true><<<grd, 256, 0, c->stream>>>(f, g, phi, c->tcol[cur], c->plane, c->P, c->Nx,
+                                                                   j0, nrows, buf);
+    else
+        rows_copy_kernel<TE, TP, false><<<grd, 256, 0, c->stream>>>(f, g, phi, c->tcol[cur], c->plane, c->P,
+                                                                    c->Nx, j0, nrows, buf);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rows_copy(bgk_ctx *c, int j0, int nrows, void *buf, bool unpack)
+{
+    unsigned char *b = static_cast<unsigned char *>(buf);
+    if (c->esz == 8) return rows_copy_t<unsigned long long, unsigned long long>(c, j0, nrows, b, unpack);
+    if (c->esz == 4)
+        return c->phisz == 8 ? rows_copy_t<unsigned int, unsigned long long>(c, j0, nrows, b, unpack)
+                             : rows_copy_t<unsigned int, unsigned int>(c, j0, nrows, b, unpack);
+    return c->phisz == 8 ? rows_copy_t<unsigned short, unsigned long long>(c, j0, nrows, b, unpack)
+                         : rows_copy_t<unsigned short, unsigned int>(c, j0, nrows, b, unpack);
 }
 
 } // namespace bgk

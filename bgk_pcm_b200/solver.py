@@ -151,6 +151,28 @@ class Solver:
     def sync(self) -> None:
         capi.check(self._lib.bgk_sync(self._h))
 
+    # -- y-slab decomposition (bgk_pcm_b200.slab) ---------------------------
+    def advance(self, n: int) -> None:
+        """n fused steps without writing the reference-layout fields."""
+        capi.check(self._lib.bgk_advance(self._h, int(n)))
+
+    def rows_bytes(self, nrows: int) -> int:
+        v = ctypes.c_size_t()
+        capi.check(self._lib.bgk_rows_bytes(self._h, int(nrows), ctypes.byref(v)))
+        return v.value
+
+    def rows_pack(self, j0: int, nrows: int, dev_ptr: int) -> None:
+        """Pack interior rows j0.. (0-based) into device memory at dev_ptr."""
+        capi.check(self._lib.bgk_rows_pack(self._h, int(j0), int(nrows), ctypes.c_void_p(dev_ptr)))
+
+    def rows_unpack(self, j0: int, nrows: int, dev_ptr: int) -> None:
+        capi.check(self._lib.bgk_rows_unpack(self._h, int(j0), int(nrows), ctypes.c_void_p(dev_ptr)))
+
+    def sums_rows(self, j0: int, nrows: int) -> np.ndarray:
+        out = np.empty(4, dtype=np.float64)
+        capi.check(self._lib.bgk_field_sums_rows(self._h, int(j0), int(nrows), _dptr(out)))
+        return out
+
     @property
     def stream(self) -> int:
         """The context's cudaStream_t as an integer handle."""

@@ -251,6 +251,41 @@ int bgk_adjoint_run(bgk_ctx *ctx, const bgk_adjoint_spec *spec, double *loss,
 int bgk_field_sums_static(const double *rho, const double *T, const double *phi, int Nx, int Ny,
                           int ld, void *stream, double *out);
 
+/* ------------------------------------------------ y-slab decomposition */
+/* A domain split into slabs of rows, one context per slab, each holding
+ * copies ("ghost rows") of its neighbours' rows on every side that is a cut
+ * rather than a wall.  The step treats a context's first and last rows as
+ * the N/S walls, so a ghost row's own update is wrong and the error moves
+ * one row inward per step; with H ghost rows a slab takes H steps and then
+ * replaces its ghost rows by the neighbours' current rows, and every real
+ * row is bit-identical to the undivided run.  No reference counterpart:
+ * the reference runs on one node (STEP_OPENMP splits loops, not the
+ * domain). */
+
+/* nsteps fused steps without writing the reference-layout fields (rho, T,
+ * u, v, phi and halos keep their values): the steps between two halo
+ * exchanges.  The populations, phi and it advance exactly as in bgk_step;
+ * the last two steps before fields are read must go through bgk_step. */
+int bgk_advance(bgk_ctx *ctx, int nsteps);
+
+/* Bytes of nrows packed rows of the step state: the 18 population planes at
+ * the context's storage size, phi, and the east T column, each section
+ * padded to 16 bytes. */
+int bgk_rows_bytes(const bgk_ctx *ctx, int nrows, size_t *bytes);
+
+/* Pack interior rows j0 .. j0+nrows-1 (0-based; reference rows j0+1 ..) of
+ * the current step state into dev_buf, or unpack dev_buf into them: device
+ * memory of the context's device, 16-byte aligned, bgk_rows_bytes long.
+ * Asynchronous on the context's stream; the rows' reference-layout fields
+ * are not updated by unpack. */
+int bgk_rows_pack(bgk_ctx *ctx, int j0, int nrows, void *dev_buf);
+int bgk_rows_unpack(bgk_ctx *ctx, int j0, int nrows, const void *dev_buf);
+
+/* bgk_field_sums over interior rows j0 .. j0+nrows-1 only (a slab's own
+ * rows, without its ghost rows); the full range gives bgk_field_sums bit
+ * for bit. */
+int bgk_field_sums_rows(bgk_ctx *ctx, int j0, int nrows, double out[4]);
+
 /* Complete binary snapshot (populations, phi, frozen boundary values, it)
  * -- unlike the reference's text dump (STEP_7/dump_out.f90:5-18), which omits
  * phi and phi_prec.  A snapshot restores into a context of the same size and
