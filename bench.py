@@ -18,8 +18,11 @@ L2, so consecutive steps never hit a warm cache.
             threads) on a bounded number of steps of the same workload
 
 `--impl reference` times that CPU implementation alone as the reference arm.
-Multi-GPU (torchrun, N ranks): every rank runs its own replica of the
-workload (weak scaling); the step has no cross-rank data path.
+Multi-GPU (torchrun, N ranks): the y-slab decomposition (bgk_pcm_b200.slab).
+The cavity grows to N x Ny rows (weak scaling: every rank owns the Ny rows
+of the workload plus ghost rows), and the ranks exchange their cut rows
+over NCCL every --halo steps.  `--decomp replicas` runs N independent
+replicas instead.
 """
 from __future__ import annotations
 
@@ -213,6 +216,79 @@ def e2e_run(params, precision, steps, device, torch):
     return ms, h2d, d2h
 
 
+def slab_timed(params, precision, steps, warmup, halo, torch, dist, sampler=None):
+    """The y-slab run of this rank (DistTransport over NCCL): device time of
+    `steps` steps on the rank's context stream, which also orders the halo
+    exchanges, with clock samples when a sampler is given."""
+    from bgk_pcm_b200.slab import DistTransport, SlabRun
+    run = SlabRun(params, halo=halo, precision=precision, transport=DistTransport())
+    run.initialization()
+    run.step(warmup)
+    run.sync()
+    stream = torch.cuda.ExternalStream(run.slabs[0].solver.stream)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks = None
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    ev0.record(stream)
+    run.step(steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    if sampler:
+        clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1)
+    dist.barrier()
+    run.close()
+    return ms, clocks
+
+
+def e2e_slab(params, precision, steps, halo, torch, dist):
+    """The end-to-end run of this rank's slab: its initial fields uploaded
+    from pinned host memory, the steps with the diagnostic cadence (sums
+    all-reduced, the probe read back every 1000 steps), its own rows of
+    rho/T/u/v/phi downloaded."""
+    from bgk_pcm_b200.slab import DistTransport, SlabRun
+    names = [f"f{k}" for k in range(9)] + [f"g{k}" for k in range(9)] + ["rho", "T", "u", "v", "phi"]
+    run = SlabRun(params, halo=halo, precision=precision, transport=DistTransport())
+    s = run.slabs[0].solver
+    s.initialization()
+    host_in = {}
+    for n in names:
+        t = torch.empty(s.field(n).shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[:] = s.field(n)
+        host_in[n] = t
+    stream = torch.cuda.ExternalStream(s.stream)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    dist.barrier()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    h2d = d2h = 0
+    for n in names:
+        s.upload(n, host_in[n].numpy())
+        h2d += host_in[n].numpy().nbytes
+    done = 0
+    while done < steps:
+        chunk = min(1000, steps - done)
+        run.step(chunk)
+        done += chunk
+        sums = run.sums()
+        probe = s.region("T", params["Nx"] // 2, 1, 1, 1)
+        d2h += sums.nbytes + probe.nbytes
+    for n in ("rho", "T", "u", "v", "phi"):
+        d2h += run.own_rows(run.slabs[0], n).nbytes
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    dist.barrier()
+    run.close()
+    return ms, h2d, d2h
+
+
 def adjoint_cost(torch, repeats=3):
     """Cost of one adjoint gradient against one forward solve on the
     differentiation workload (512^2, Ra 1e5, 2000 steps, 64 probes,
@@ -264,6 +340,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward cost leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--decomp", default="slab", choices=["slab", "replicas"],
+                    help="N > 1: y-slab decomposition of one N-times taller cavity, or N replicas")
+    ap.add_argument("--halo", type=int, default=8, help="ghost rows per cut (steps between exchanges)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -318,7 +397,13 @@ def main():
         s.close()
         return ms, clocks
 
-    ms, clocks = run_form(args.precision, False, args.steps, args.warmup, sample_clocks=True)
+    slab = world > 1 and args.decomp == "slab"
+    gparams = dict(params, Ny=Ny * world) if slab else params
+    if slab:
+        ms, clocks = slab_timed(gparams, args.precision, args.steps, args.warmup, args.halo, torch, dist,
+                                ClockSampler(local))
+    else:
+        ms, clocks = run_form(args.precision, False, args.steps, args.warmup, sample_clocks=True)
     ms = max_over_ranks(ms, dist, "cuda")
     value = whole_job_glups(nodes, args.steps, world, ms)
     hbm, hbm_kind = peaks()
@@ -369,7 +454,10 @@ def main():
 
     e2e = None
     if not args.no_e2e:
-        e_ms, h2d, d2h = e2e_run(params, args.precision, args.steps, local, torch)
+        if slab:
+            e_ms, h2d, d2h = e2e_slab(gparams, args.precision, args.steps, args.halo, torch, dist)
+        else:
+            e_ms, h2d, d2h = e2e_run(params, args.precision, args.steps, local, torch)
         e_ms = max_over_ranks(e_ms, dist, "cuda")
         e2e = {"value": whole_job_glups(nodes, args.steps, world, e_ms), "unit": "GLUPS",
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
@@ -393,7 +481,10 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": args.precision,
             "data": "synthetic: the reference's initial condition on the generated input.dat",
             "config": {"workload": args.workload, "Nx": Nx, "Ny": Ny, "Ra": wl["Ra"], "Pr": wl["Pr"],
-                       "Ste": wl["Ste"], "precision": args.precision, "parallelism": f"replicas{world}",
+                       "Ste": wl["Ste"], "precision": args.precision,
+                       "parallelism": (f"yslab{world}" if slab else f"replicas{world}"),
+                       "global_Ny": Ny * world if slab else Ny,
+                       "halo_rows": args.halo if slab else None,
                        "l2": "inputs larger than L2 (A/B populations %.0f MB > 126 MB)"
                              % (2 * 18 * {"f64": 8, "f32": 4, "f16": 2, "f32x": 4}[args.precision] * nodes / 1e6)},
             "hbm_gbs": value / world * bpn,
@@ -407,7 +498,9 @@ def main():
             "e2e": e2e,
             "cpu_baseline": cpu,
             "cpu_baseline_serial": cpu1,
-            "gpu_launches": args.steps + 1,
+            # fused steps + the final halo fill; with slabs, rank 0 (one
+            # cut) also packs and unpacks its rows once per exchange
+            "gpu_launches": args.steps + 1 + (2 * -(-args.steps // args.halo) if slab else 0),
         }
         print(json.dumps(line), flush=True)
     if dist:

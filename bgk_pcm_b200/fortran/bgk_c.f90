@@ -178,6 +178,40 @@ module bgk_c
        type(c_ptr), intent(out) :: stream
        integer(c_int) :: rc
      end function
+     ! y-slab decomposition: steps between halo exchanges and the packed
+     ! ghost rows (device buffers, e.g. from the host's MPI/NCCL layer)
+     function bgk_advance(ctx, nsteps) bind(c, name="bgk_advance") result(rc)
+       import :: c_int, c_ptr
+       type(c_ptr), value :: ctx
+       integer(c_int), value :: nsteps
+       integer(c_int) :: rc
+     end function
+     function bgk_rows_bytes(ctx, nrows, bytes) bind(c, name="bgk_rows_bytes") result(rc)
+       import :: c_int, c_ptr, c_size_t
+       type(c_ptr), value :: ctx
+       integer(c_int), value :: nrows
+       integer(c_size_t), intent(out) :: bytes
+       integer(c_int) :: rc
+     end function
+     function bgk_rows_pack(ctx, j0, nrows, dev_buf) bind(c, name="bgk_rows_pack") result(rc)
+       import :: c_int, c_ptr
+       type(c_ptr), value :: ctx, dev_buf
+       integer(c_int), value :: j0, nrows
+       integer(c_int) :: rc
+     end function
+     function bgk_rows_unpack(ctx, j0, nrows, dev_buf) bind(c, name="bgk_rows_unpack") result(rc)
+       import :: c_int, c_ptr
+       type(c_ptr), value :: ctx, dev_buf
+       integer(c_int), value :: j0, nrows
+       integer(c_int) :: rc
+     end function
+     function bgk_field_sums_rows(ctx, j0, nrows, sums) bind(c, name="bgk_field_sums_rows") result(rc)
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: ctx
+       integer(c_int), value :: j0, nrows
+       real(c_double), dimension(4), intent(out) :: sums
+       integer(c_int) :: rc
+     end function
      function bgk_last_error() bind(c, name="bgk_last_error") result(msg)
        import :: c_ptr
        type(c_ptr) :: msg
