@@ -48,7 +48,8 @@ EXPORTS = [
     "bgk_phase_field", "bgk_forces", "bgk_collision", "bgk_moments", "bgk_upload",
     "bgk_download", "bgk_download_region", "bgk_field_sums", "bgk_get_it", "bgk_set_it",
     "bgk_set_tin", "bgk_sync", "bgk_get_stream", "bgk_save", "bgk_load", "bgk_adjoint_run",
-    "bgk_field_sums_static",
+    "bgk_field_sums_static", "bgk_advance", "bgk_rows_bytes", "bgk_rows_pack", "bgk_rows_unpack",
+    "bgk_field_sums_rows",
 ]
 
 STATIC_SUMS_MAX_NY = 32768
