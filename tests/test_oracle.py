@@ -151,3 +151,15 @@ def test_workload_mapping():
         d = inputs.diag_numbers(v)
         assert abs(d["Ra"] / w["Ra"] - 1) < 1e-12 and abs(d["Pr"] - w["Pr"]) < 1e-12
         assert v["Nx"] == w["Nx"] and v["Ny"] == w["Ny"] and v["stefan_number"] == w["Ste"]
+
+
+def test_thread_sweep_matches_across_thread_counts(oracle_mod):
+    """oracle/thread_sweep.py, the counterpart of UTIL/RunMe_thread.sh: the
+    same fields (md5) at every thread count, and a positive rate."""
+    from oracle import thread_sweep
+    p = small_params(40, 28)
+    rows = thread_sweep.threads_sweep(p, 6, 4)
+    assert [r["threads"] for r in rows] == [4, 2, 1]
+    assert len({r["md5"] for r in rows}) == 1
+    assert all(r["mlups"] > 0 for r in rows)
+    assert thread_sweep.thread_counts(6) == [6, 4, 2, 1]
