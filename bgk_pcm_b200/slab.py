@@ -202,6 +202,10 @@ class DistTransport:
         self.rank = dist.get_rank(group)
         self.world = dist.get_world_size(group)
 
+    def peer(self, r: int) -> int:
+        """Global rank of the group's rank r (the slab index)."""
+        return r if self.group is None else self.dist.get_global_rank(self.group, r)
+
     def exchange(self, slabs) -> None:
         (s,) = slabs
         dist, r, n = self.dist, self.rank, self.world
@@ -209,11 +213,11 @@ class DistTransport:
         with ctx:
             ops = []
             if r > 0:
-                ops.append(dist.P2POp(dist.isend, s.pack("lo"), r - 1, self.group))
-                ops.append(dist.P2POp(dist.irecv, s.recv_buffer("lo"), r - 1, self.group))
+                ops.append(dist.P2POp(dist.isend, s.pack("lo"), self.peer(r - 1), self.group))
+                ops.append(dist.P2POp(dist.irecv, s.recv_buffer("lo"), self.peer(r - 1), self.group))
             if r < n - 1:
-                ops.append(dist.P2POp(dist.isend, s.pack("hi"), r + 1, self.group))
-                ops.append(dist.P2POp(dist.irecv, s.recv_buffer("hi"), r + 1, self.group))
+                ops.append(dist.P2POp(dist.isend, s.pack("hi"), self.peer(r + 1), self.group))
+                ops.append(dist.P2POp(dist.irecv, s.recv_buffer("hi"), self.peer(r + 1), self.group))
             if ops:
                 for w in dist.batch_isend_irecv(ops):
                     w.wait()
@@ -291,7 +295,7 @@ class SlabRun:
         if isinstance(self.transport, DistTransport):
             d = self.transport.dist
             gathered = [None] * self.transport.world if self.transport.rank == 0 else None
-            d.gather_object(parts, gathered, dst=0, group=self.transport.group)
+            d.gather_object(parts, gathered, dst=self.transport.peer(0), group=self.transport.group)
             if self.transport.rank != 0:
                 return None
             parts = [x for g in gathered for x in g]
