@@ -41,3 +41,16 @@ def test_create_fails_loudly_without_gpu(lib):
     from conftest import small_params
     with pytest.raises(BGKError, match="BGK_ERR_CUDA.*no CPU path"):
         Solver(small_params())
+
+
+def test_slab_entry_points_reject_null_arguments(lib):
+    """The y-slab entry points check their arguments before any CUDA call."""
+    size = ctypes.c_size_t()
+    out = (ctypes.c_double * 4)()
+    fake = ctypes.c_void_p(4096)
+    assert lib.bgk_advance(None, 3) == -1
+    assert lib.bgk_rows_bytes(None, 2, ctypes.byref(size)) == -1
+    assert lib.bgk_rows_pack(None, 0, 2, fake) == -1
+    assert lib.bgk_rows_unpack(None, 0, 2, fake) == -1
+    assert lib.bgk_field_sums_rows(None, 0, 2, out) == -1
+    assert "null" in lib.bgk_last_error().decode()
