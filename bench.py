@@ -249,8 +249,8 @@ def slab_timed(params, precision, steps, warmup, halo, torch, dist, sampler=None
 def e2e_slab(params, precision, steps, halo, torch, dist):
     """The end-to-end run of this rank's slab: its initial fields uploaded
     from pinned host memory, the steps with the diagnostic cadence (sums
-    all-reduced, the probe read back every 1000 steps), its own rows of
-    rho/T/u/v/phi downloaded."""
+    all-reduced, the probe read back every 1000 steps), and its
+    rho/T/u/v/phi downloaded (the slab's whole reference-layout fields)."""
     from bgk_pcm_b200.slab import DistTransport, SlabRun
     names = [f"f{k}" for k in range(9)] + [f"g{k}" for k in range(9)] + ["rho", "T", "u", "v", "phi"]
     run = SlabRun(params, halo=halo, precision=precision, transport=DistTransport())
@@ -280,7 +280,7 @@ def e2e_slab(params, precision, steps, halo, torch, dist):
         probe = s.region("T", params["Nx"] // 2, 1, 1, 1)
         d2h += sums.nbytes + probe.nbytes
     for n in ("rho", "T", "u", "v", "phi"):
-        d2h += run.own_rows(run.slabs[0], n).nbytes
+        d2h += run.slabs[0].local_field(n).nbytes      # the slab's whole field crosses
     ev1.record(stream)
     ev1.synchronize()
     ms = ev0.elapsed_time(ev1)
