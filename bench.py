@@ -483,7 +483,8 @@ def main():
             "data": "synthetic: the reference's initial condition on the generated input.dat",
             "config": {"workload": args.workload, "Nx": Nx, "Ny": Ny, "Ra": wl["Ra"], "Pr": wl["Pr"],
                        "Ste": wl["Ste"], "precision": args.precision,
-                       "parallelism": (f"yslab{world}" if slab else f"replicas{world}"),
+                       "parallelism": (f"yslab{world}" if slab else
+                                       (f"replicas{world}" if world > 1 else "single-gpu")),
                        "global_Ny": Ny * world if slab else Ny,
                        "halo_rows": args.halo if slab else None,
                        "l2": "inputs larger than L2 (A/B populations %.0f MB > 126 MB)"
