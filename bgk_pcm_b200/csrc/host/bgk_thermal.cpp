@@ -80,7 +80,7 @@ std::string fE(double x, int w, int d)
 /* gfortran list-directed REAL(8) (17 significant digits). */
 std::string flist(double x)
 {
-    char out[64];
+    char out[96];                    /* room for tmp (64) plus the exponent */
     double ax = std::fabs(x);
     if (x != 0.0 && (ax < 0.1 || ax >= 1e16)) {
         char tmp[64];
