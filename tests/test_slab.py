@@ -10,7 +10,6 @@ slab exchanges every per-node array of its rows, not only the fused step's
 state."""
 from __future__ import annotations
 
-import os
 import socket
 
 import numpy as np
@@ -224,3 +223,48 @@ def test_gloo_ranks_match_undivided_oracle(oracle_mod, world, halo, steps):
     for r in range(world):                       # all_reduce: every rank holds the same sums
         np.testing.assert_array_equal(res[r][1], res[0][1])
     assert res[0][1][3] == float((ref["phi"][1:-1, 1:-1] > 0).sum())
+
+
+def _subgroup_main(rank, world, port, q):
+    import datetime
+    import sys
+    sys.path.insert(0, str(ROOT))
+    sys.path.insert(0, str(ROOT / "tests"))
+    import torch.distributed as dist
+    from bgk_pcm_b200.slab import DistTransport, SlabRun
+    from test_slab import OracleSlab, _params
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        group = dist.new_group([1, 2])              # every rank takes part in new_group
+        if rank in (1, 2):
+            params = _params()
+            run = SlabRun(params, halo=2, transport=DistTransport(group),
+                          slab_factory=lambda plan, r: OracleSlab(plan, r, params))
+            run.initialization()
+            run.step(7)
+            phi = run.field("phi")
+            run.close()
+            q.put((rank, phi))
+        else:
+            q.put((rank, None))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_subgroup_addresses_peers_by_global_rank(oracle_mod):
+    """Slabs on ranks 1 and 2 of a 3-rank world, through a subgroup: the
+    group's rank 0 (global rank 1) gathers the field."""
+    world, port = 3, _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_subgroup_main, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=180) for _ in range(world))
+    for p in procs:
+        p.join(60)
+        assert p.exitcode == 0
+    ref = _undivided(_params(), 7)
+    assert res[0] is None and res[2] is None
+    np.testing.assert_array_equal(res[1], ref["phi"])
