@@ -112,13 +112,44 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_oracle_rate(params, budget_s: float = 15.0, max_steps: int = 400, threads: int = 0, warmup: int = 2):
+def host_cpu() -> dict:
+    """The host's CPU model, the logical CPUs this process may run on, and
+    the physical cores among them (distinct (package, core) pairs of
+    /proc/cpuinfo; SMT siblings share a core)."""
+    try:
+        allowed = os.sched_getaffinity(0)
+    except (AttributeError, OSError):
+        allowed = set(range(os.cpu_count() or 1))
+    model, cores = None, set()
+    try:
+        blocks = Path("/proc/cpuinfo").read_text().split("\n\n")
+    except OSError:
+        blocks = []
+    for block in blocks:
+        d = {}
+        for ln in block.splitlines():
+            if ":" in ln:
+                k, v = ln.split(":", 1)
+                d[k.strip()] = v.strip()
+        if "processor" not in d:
+            continue
+        model = model or d.get("model name")
+        p = int(d["processor"])
+        if p in allowed:
+            cores.add((d.get("physical id", "0"), d.get("core id", str(p))))
+    return {"model": model, "logical_cpus": len(allowed), "physical_cores": len(cores) or len(allowed)}
+
+
+def cpu_oracle_rate(params, budget_s: float = 15.0, max_steps: int = 400, threads: int = 0, warmup: int = 2,
+                    tanh: str = "device"):
     """GLUPS of the CPU oracle on whole steps of `params`, with `threads`
-    OpenMP threads (0: all host threads; 1: the serial STEP_7 restatement).
-    `warmup` untimed steps (at least 2) also size the timed sample."""
+    OpenMP threads (0: one per physical core, where the thread sweep of the
+    oracle peaks; 1: the serial STEP_7 restatement).  `warmup` untimed steps
+    (at least 2) also size the timed sample.  tanh: "portable" (the same
+    function as the GPU's portable form) or the host libm's."""
     from oracle import pyoracle
-    threads = threads or os.cpu_count() or 1
-    o = pyoracle.Oracle(params, threads=threads)
+    threads = threads or host_cpu()["physical_cores"]
+    o = pyoracle.Oracle(params, threads=threads, tanh="portable" if tanh == "portable" else "libm")
     o.initialization()
     w = max(2, warmup)
     t0 = time.perf_counter()
@@ -169,7 +200,7 @@ def time_steps(solver, steps: int, torch):
     return start.elapsed_time(end)
 
 
-def e2e_run(params, precision, steps, device, torch):
+def e2e_run(params, precision, steps, device, torch, tanh="portable"):
     """Public-API run with host buffers: upload, steps + diag cadence, download."""
     import numpy as np
 
@@ -177,7 +208,7 @@ def e2e_run(params, precision, steps, device, torch):
     Nx, Ny = params["Nx"], params["Ny"]
     shape = (Ny + 2, Nx + 2)
     names = [f"f{k}" for k in range(9)] + [f"g{k}" for k in range(9)] + ["rho", "T", "u", "v", "phi"]
-    src = Solver(params, precision=precision, device=device)
+    src = Solver(params, precision=precision, device=device, tanh=tanh)
     src.initialization()
     host_in = {}
     for n in names:
@@ -187,7 +218,7 @@ def e2e_run(params, precision, steps, device, torch):
         host_in[n] = (t, a)
     src.close()
     outs = {n: torch.empty(shape, dtype=torch.float64, pin_memory=True) for n in ("rho", "T", "u", "v", "phi")}
-    s = Solver(params, precision=precision, device=device)
+    s = Solver(params, precision=precision, device=device, tanh=tanh)
     stream = torch.cuda.ExternalStream(s.stream)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -216,12 +247,12 @@ def e2e_run(params, precision, steps, device, torch):
     return ms, h2d, d2h
 
 
-def slab_timed(params, precision, steps, warmup, halo, torch, dist, sampler=None):
+def slab_timed(params, precision, steps, warmup, halo, torch, dist, sampler=None, tanh="portable"):
     """The y-slab run of this rank (DistTransport over NCCL): device time of
     `steps` steps on the rank's context stream, which also orders the halo
     exchanges, with clock samples when a sampler is given."""
     from bgk_pcm_b200.slab import DistTransport, SlabRun
-    run = SlabRun(params, halo=halo, precision=precision, transport=DistTransport())
+    run = SlabRun(params, halo=halo, precision=precision, transport=DistTransport(), tanh=tanh)
     run.initialization()
     run.step(warmup)
     run.sync()
@@ -246,14 +277,14 @@ def slab_timed(params, precision, steps, warmup, halo, torch, dist, sampler=None
     return ms, clocks
 
 
-def e2e_slab(params, precision, steps, halo, torch, dist):
+def e2e_slab(params, precision, steps, halo, torch, dist, tanh="portable"):
     """The end-to-end run of this rank's slab: its initial fields uploaded
     from pinned host memory, the steps with the diagnostic cadence (sums
     all-reduced, the probe read back every 1000 steps), and its
     rho/T/u/v/phi downloaded (the slab's whole reference-layout fields)."""
     from bgk_pcm_b200.slab import DistTransport, SlabRun
     names = [f"f{k}" for k in range(9)] + [f"g{k}" for k in range(9)] + ["rho", "T", "u", "v", "phi"]
-    run = SlabRun(params, halo=halo, precision=precision, transport=DistTransport())
+    run = SlabRun(params, halo=halo, precision=precision, transport=DistTransport(), tanh=tanh)
     s = run.slabs[0].solver
     s.initialization()
     host_in = {}
@@ -289,6 +320,24 @@ def e2e_slab(params, precision, steps, halo, torch, dist):
     return ms, h2d, d2h
 
 
+def fp64_divergence(params, device, tanh_a, tanh_b, fma_b, steps=200) -> float:
+    """Largest |difference| over rho, T, u, v, phi (halos included) between
+    the headline FP64 form (tanh_a, exact operation order) and a variant
+    (tanh_b, fma_b) after the same `steps` steps of the workload.  0 means
+    bit-identical; the headline form with the portable tanh is bit-identical
+    to the oracle (the parity tests)."""
+    import numpy as np
+
+    from bgk_pcm_b200 import Solver
+    out = []
+    for tanh, fma in ((tanh_a, False), (tanh_b, fma_b)):
+        with Solver(params, precision="f64", tanh=tanh, fma=fma, device=device) as s:
+            s.initialization()
+            s.step(steps)
+            out.append({n: s.field(n) for n in ("rho", "T", "u", "v", "phi")})
+    return {"steps": steps, "max_abs": max(float(np.abs(out[0][n] - out[1][n]).max()) for n in out[0])}
+
+
 def adjoint_cost(torch, repeats=3):
     """Cost of one adjoint gradient against one forward solve on the
     differentiation workload (512^2, Ra 1e5, 2000 steps, 64 probes,
@@ -305,24 +354,35 @@ def adjoint_cost(torch, repeats=3):
             "timing": "wall clock, synchronised, best of %d, on an existing context" % repeats}
 
 
+def bench_config(args, params, wl) -> dict:
+    """The workload, identical in both arms' lines."""
+    esz = {"f64": 8, "f32": 4, "f16": 2, "f32x": 4}[args.precision]
+    nodes = params["Nx"] * params["Ny"]
+    return {"workload": args.workload, "Nx": params["Nx"], "Ny": params["Ny"], "Ra": wl["Ra"], "Pr": wl["Pr"],
+            "Ste": wl["Ste"], "precision": args.precision, "tanh": args.tanh,
+            "l2": "inputs larger than L2 (A/B populations %.0f MB > 126 MB), no flush" % (2 * 18 * esz * nodes / 1e6)}
+
+
 def run_reference(args, params, wl):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     w = max(2, args.warmup)
+    cpu = host_cpu()
     glups, n, threads = cpu_oracle_rate(params, budget_s=min(60.0, 5.0 + 0.5 * args.steps), max_steps=args.steps,
-                                        warmup=w)
+                                        warmup=w, tanh=args.tanh)
     line = {
         "impl": "reference", "metric": METRIC, "value": glups, "unit": "GLUPS", "n_gpus": args.gpus,
         "steps": n, "warmup": w, "ms_per_step": params["Nx"] * params["Ny"] / glups / 1e6,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (the reference's initial condition on the generated input.dat)",
-        "config": {"workload": args.workload, "Nx": params["Nx"], "Ny": params["Ny"], "Ra": wl["Ra"],
-                   "Pr": wl["Pr"], "Ste": wl["Ste"], "precision": "f64"},
+        "config": bench_config(args, params, wl),
         "cpu_baseline": {"value": glups, "unit": "GLUPS", "cores": threads, "kind": "port",
+                         "threads": threads, "physical_cores": cpu["physical_cores"],
+                         "logical_cpus": cpu["logical_cpus"], "cpu_model": cpu["model"],
                          "sample": f"{n} whole steps of the {params['Nx']}x{params['Ny']} grid; C restatement of "
-                                   "STEP_7 (OpenMP, bit-identical to serial); the Fortran reference cannot be "
-                                   "compiled in this image"},
+                                   "STEP_7 (OpenMP over the j loops, one thread per physical core, bit-identical "
+                                   "to serial); the Fortran reference cannot be compiled in this image"},
         "e2e": {"value": glups, "unit": "GLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -336,7 +396,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cavity2048_ra1e6")
     ap.add_argument("--precision", default="f64", choices=["f64", "f32", "f16", "f32x"])
-    ap.add_argument("--forms", default="f64fma,f32,f16,f32x", help="extra forms timed beside the headline (comma list)")
+    ap.add_argument("--tanh", default="portable", choices=["portable", "device"],
+                    help="phase-field tanh: the portable one (bit-identical to the oracle) or CUDA's")
+    ap.add_argument("--forms", default="f64device,f64fma,f32,f16,f32x",
+                    help="extra forms timed beside the headline (comma list)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward cost leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
@@ -378,8 +441,8 @@ def main():
         if dist:
             dist.barrier()
 
-    def run_form(precision, fma, steps, warmup, sample_clocks=False):
-        s = Solver(params, precision=precision, fma=fma, device=local)
+    def run_form(precision, fma, steps, warmup, sample_clocks=False, tanh=args.tanh):
+        s = Solver(params, precision=precision, fma=fma, device=local, tanh=tanh)
         s.initialization()
         s.step(warmup)
         s.sync()
@@ -402,7 +465,7 @@ def main():
     gparams = dict(params, Ny=Ny * world) if slab else params
     if slab:
         ms, clocks = slab_timed(gparams, args.precision, args.steps, args.warmup, args.halo, torch, dist,
-                                ClockSampler(local))
+                                ClockSampler(local), tanh=args.tanh)
     else:
         ms, clocks = run_form(args.precision, False, args.steps, args.warmup, sample_clocks=True)
     ms = max_over_ranks(ms, dist, "cuda")
@@ -416,17 +479,27 @@ def main():
     forms = {}
     # extra forms on a single process only: a form that fails on one rank
     # must not leave the ranks at different collective steps
+    # name -> (precision, FMA contraction, tanh); the reduced-precision forms
+    # are not bit-exact with anything, so they use CUDA's tanh(f)
+    form_spec = {"f64device": ("f64", False, "device"), "f64fma": ("f64", True, args.tanh),
+                 "f32": ("f32", False, "device"), "f16": ("f16", False, "device"),
+                 "f32x": ("f32x", False, "device")}
     for form in [f for f in args.forms.split(",") if f and f != "none" and world == 1]:
-        prec, fma = ("f64", True) if form == "f64fma" else (form, False)
+        if form not in form_spec:
+            forms[form] = {"error": "unknown form"}
+            continue
+        prec, fma, tanh = form_spec[form]
         try:
-            fms, _ = run_form(prec, fma, max(args.steps // 4, 100), args.warmup)
+            fms, _ = run_form(prec, fma, max(args.steps // 4, 100), args.warmup, tanh=tanh)
         except Exception as exc:  # a form that is not available is reported, not fatal
             forms[form] = {"error": str(exc)}
             continue
         g = nodes * max(args.steps // 4, 100) / (fms / 1e3) / 1e9
         b = BYTES_PER_NODE[prec]
-        forms[form] = {"glups": g, "hbm_gbs": g * b, "frac_of_measured_hbm": g * b / hbm,
-                       "bytes_per_node": b, "speedup_vs_headline": g / (value / world)}
+        forms[form] = {"glups": g, "hbm_gbs": g * b, "frac_of_measured_hbm": g * b / hbm, "bytes_per_node": b,
+                       "speedup_vs_headline": g / (value / world), "tanh": tanh, "fma": fma}
+        if prec == "f64" and args.precision == "f64":
+            forms[form]["max_abs_vs_headline"] = fp64_divergence(params, local, args.tanh, tanh, fma)
 
     # the precision-form workload (4096^2, Ra 1e7): FP32 storage against FP64
     precision_cfg = None
@@ -456,9 +529,9 @@ def main():
     e2e = None
     if not args.no_e2e:
         if slab:
-            e_ms, h2d, d2h = e2e_slab(gparams, args.precision, args.steps, args.halo, torch, dist)
+            e_ms, h2d, d2h = e2e_slab(gparams, args.precision, args.steps, args.halo, torch, dist, tanh=args.tanh)
         else:
-            e_ms, h2d, d2h = e2e_run(params, args.precision, args.steps, local, torch)
+            e_ms, h2d, d2h = e2e_run(params, args.precision, args.steps, local, torch, tanh=args.tanh)
         e_ms = max_over_ranks(e_ms, dist, "cuda")
         e2e = {"value": whole_job_glups(nodes, args.steps, world, e_ms), "unit": "GLUPS",
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
@@ -467,11 +540,13 @@ def main():
 
     cpu = cpu1 = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        glups, n, threads = cpu_oracle_rate(params)
-        cpu = {"value": glups, "unit": "GLUPS", "cores": threads, "kind": "port",
+        hc = host_cpu()
+        glups, n, threads = cpu_oracle_rate(params, tanh=args.tanh)
+        cpu = {"value": glups, "unit": "GLUPS", "cores": threads, "kind": "port", "threads": threads,
+               "physical_cores": hc["physical_cores"], "logical_cpus": hc["logical_cpus"], "cpu_model": hc["model"],
                "sample": f"{n} whole steps of the {Nx}x{Ny} grid, C restatement of STEP_7 with OpenMP "
-                         "(STEP_OPENMP's parallelisation; bit-identical to serial)"}
-        glups1, n1, _ = cpu_oracle_rate(params, budget_s=8.0, threads=1)
+                         "(STEP_OPENMP's parallelisation, one thread per physical core; bit-identical to serial)"}
+        glups1, n1, _ = cpu_oracle_rate(params, budget_s=8.0, threads=1, tanh=args.tanh)
         cpu1 = {"value": glups1, "unit": "GLUPS", "cores": 1, "kind": "port",
                 "sample": f"{n1} whole steps of the {Nx}x{Ny} grid, serial C restatement of STEP_7"}
 
@@ -481,14 +556,11 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": args.precision,
             "data": "synthetic: the reference's initial condition on the generated input.dat",
-            "config": {"workload": args.workload, "Nx": Nx, "Ny": Ny, "Ra": wl["Ra"], "Pr": wl["Pr"],
-                       "Ste": wl["Ste"], "precision": args.precision,
-                       "parallelism": (f"yslab{world}" if slab else
+            "config": bench_config(args, params, wl),
+            "layout": {"parallelism": (f"yslab{world}" if slab else
                                        (f"replicas{world}" if world > 1 else "single-gpu")),
                        "global_Ny": Ny * world if slab else Ny,
-                       "halo_rows": args.halo if slab else None,
-                       "l2": "inputs larger than L2 (A/B populations %.0f MB > 126 MB)"
-                             % (2 * 18 * {"f64": 8, "f32": 4, "f16": 2, "f32x": 4}[args.precision] * nodes / 1e6)},
+                       "halo_rows": args.halo if slab else None},
             "hbm_gbs": value / world * bpn,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic, "peak_kind": hbm_kind,

@@ -693,6 +693,9 @@ static int rows_copy(bgk_ctx *c, int j0, int nrows, const void *buf, bool unpack
     if (j0 < 0 || nrows < 1 || (long long)j0 + nrows > c->Ny)
         return fail(BGK_ERR_ARG, "rows %d..%d outside 0..%d", j0, j0 + nrows - 1, c->Ny - 1);
     if ((uintptr_t)buf & 15u) return fail(BGK_ERR_ARG, "row buffer is not 16-byte aligned");
+    if (!all_bc4(c->p))
+        return fail(BGK_ERR_UNSUPPORTED, "packed rows belong to the fused step, which implements the no-slip "
+                                         "code 4 on every wall");
     int rc = set_device(c);
     if (rc) return rc;
     cudaPointerAttributes at;

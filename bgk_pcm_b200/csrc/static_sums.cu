@@ -14,16 +14,20 @@
  *
  * Scratch: g_row_partials, a file-scope __device__ array of
  * 4 * BGK_STATIC_SUMS_MAX_NY doubles (1 MiB per device).  Its device address
- * is looked up once per device with cudaGetSymbolAddress and cached.  Every
+ * is looked up with cudaGetSymbolAddress on the first call in each CUDA
+ * context of a device and cached under that context's unique id, so a
+ * context that replaces the old one (cudaDeviceReset, or a caller's own
+ * driver-API context) gets its own lookup instead of a stale address.  Every
  * slot a call reads was written earlier by the same call, so no part of the
  * scratch has to start at zero and nothing is cleared between calls.  All
  * calls on one device share the array: calls that can overlap in time race.
  */
-#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 
+#include <cuda.h>            /* driver types only; entry points come from the runtime */
 #include <cuda_runtime.h>
 
 #include "bgk_pcm.h"
@@ -37,7 +41,70 @@ constexpr int MAX_DEVICES = 64;
 
 static __device__ __align__(256) double g_row_partials[4 * BGK_STATIC_SUMS_MAX_NY];
 
-std::atomic<double *> g_partials_addr[MAX_DEVICES];
+/* The scratch address per device, valid for the context it was looked up in. */
+struct ScratchAddr {
+    unsigned long long ctx_id = 0;
+    double *ptr = nullptr;
+};
+ScratchAddr g_partials_addr[MAX_DEVICES];
+std::mutex g_partials_mu;
+
+/* Unique id of the calling thread's current CUDA context (0 if none), via
+ * the driver entry points the runtime hands out, so the library needs no
+ * link dependency on the driver library. */
+unsigned long long current_ctx_id()
+{
+    using GetCurrent = CUresult (*)(CUcontext *);
+    using GetId = CUresult (*)(CUcontext, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+        cudaGetLastError();
+    });
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+    if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+/* The scratch address in the current context of device dev: looked up on
+ * the first call in that context, cached afterwards. */
+int scratch_address(int dev, double **out)
+{
+    std::lock_guard<std::mutex> lock(g_partials_mu);
+    ScratchAddr &a = g_partials_addr[dev];
+    const unsigned long long id = current_ctx_id();
+    if (a.ptr && id != 0 && a.ctx_id == id) {
+        *out = a.ptr;
+        return BGK_OK;
+    }
+    void *addr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&addr, g_row_partials);
+    if (e != cudaSuccess || !addr) {
+        cudaGetLastError();
+        char msg[200];
+        std::snprintf(msg, sizeof msg, "bgk_field_sums_static: cudaGetSymbolAddress failed: %s",
+                      cudaGetErrorString(e));
+        return bgk_internal_fail(BGK_ERR_CUDA, msg);
+    }
+    /* the lookup makes the context current if nothing was; cache under its id
+     * (an id of 0, no context known, is never a cache hit) */
+    a.ctx_id = id != 0 ? id : current_ctx_id();
+    a.ptr = static_cast<double *>(addr);
+    *out = a.ptr;
+    return BGK_OK;
+}
 
 __device__ __forceinline__ double warp_total(double v)
 {
@@ -143,20 +210,8 @@ extern "C" int bgk_field_sums_static(const double *rho, const double *T, const d
         (rc = check_device_pointer(phi, dev, "phi")) || (rc = check_device_pointer(out, dev, "out")))
         return rc;
 
-    double *part = g_partials_addr[dev].load(std::memory_order_acquire);
-    if (!part) {
-        void *addr = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&addr, g_row_partials);
-        if (e != cudaSuccess || !addr) {
-            cudaGetLastError();
-            char msg[200];
-            std::snprintf(msg, sizeof msg, "bgk_field_sums_static: cudaGetSymbolAddress failed: %s",
-                          cudaGetErrorString(e));
-            return bgk_internal_fail(BGK_ERR_CUDA, msg);
-        }
-        part = static_cast<double *>(addr);
-        g_partials_addr[dev].store(part, std::memory_order_release);
-    }
+    double *part = nullptr;
+    if ((rc = scratch_address(dev, &part))) return rc;
 
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     row_sums_kernel<<<Ny, ROW_THREADS, 0, s>>>(rho, T, phi, Nx, Ny, (long long)ld, part);

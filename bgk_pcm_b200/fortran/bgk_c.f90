@@ -8,11 +8,16 @@ module bgk_c
   implicit none
 
   integer(c_int), parameter :: BGK_OK = 0
+  integer(c_int), parameter :: BGK_ERR_ARG = -1, BGK_ERR_UNSUPPORTED = -2, BGK_ERR_CUDA = -3, &
+                               BGK_ERR_OOM = -4, BGK_ERR_STATE = -5, BGK_ERR_IO = -6, BGK_ERR_NONFINITE = -7
   integer(c_int), parameter :: BGK_PREC_F64 = 0, BGK_PREC_F32 = 1, BGK_PREC_F16 = 2, BGK_PREC_F32X = 3
   integer(c_int), parameter :: BGK_TANH_DEVICE = 0, BGK_TANH_PORTABLE = 1
   integer(c_int), parameter :: BGK_FIELD_F0 = 0, BGK_FIELD_G0 = 9
   integer(c_int), parameter :: BGK_FIELD_RHO = 18, BGK_FIELD_T = 19, BGK_FIELD_U = 20, BGK_FIELD_V = 21
   integer(c_int), parameter :: BGK_FIELD_PHI = 22, BGK_FIELD_PHI_PREC = 23
+  integer(c_int), parameter :: BGK_FIELD_RHO2 = 24, BGK_FIELD_T2 = 25, BGK_FIELD_U2 = 26, BGK_FIELD_V2 = 27
+  integer(c_int), parameter :: BGK_FIELD_FP0 = 28, BGK_FIELD_GP0 = 37, BGK_NFIELDS = 46
+  integer(c_int), parameter :: BGK_STATIC_SUMS_MAX_NY = 32768
 
   type, bind(c) :: bgk_params
      integer(c_int) :: iter, noutput, dump, Nx, Ny
@@ -210,6 +215,16 @@ module bgk_c
        type(c_ptr), value :: ctx
        integer(c_int), value :: j0, nrows
        real(c_double), dimension(4), intent(out) :: sums
+       integer(c_int) :: rc
+     end function
+     ! interior sums over the caller's own device arrays, with no allocation
+     ! (rho, T, phi, out: device addresses, e.g. from CUDA Fortran's c_devloc)
+     function bgk_field_sums_static(rho, T, phi, Nx, Ny, ld, stream, out) &
+          bind(c, name="bgk_field_sums_static") result(rc)
+       import :: c_int, c_ptr
+       type(c_ptr), value :: rho, T, phi
+       integer(c_int), value :: Nx, Ny, ld
+       type(c_ptr), value :: stream, out
        integer(c_int) :: rc
      end function
      function bgk_last_error() bind(c, name="bgk_last_error") result(msg)

@@ -234,6 +234,13 @@ class SlabRun:
     def __init__(self, params: dict, nslabs: int | None = None, halo: int = 4, precision: str = "f64",
                  transport=None, slab_factory=None, devices=None, **solver_kw):
         self.params = dict(params)
+        walls = [self.params.get(k, 4) for k in ("westBC", "eastBC", "northBC", "southBC")]
+        if any(int(w) != 4 for w in walls):
+            # the fused step (bgk_step, bgk_advance) implements only the
+            # no-slip code 4, and a cut is only a wall of code 4 seen from a
+            # slab: an inflow or pressure code would be built from the slab's
+            # own rows (STEP_7/BC_f.f90:7-60) and be wrong on every slab
+            raise ValueError(f"SlabRun needs the no-slip code 4 on every wall, got W/E/N/S = {walls}")
         self.transport = transport or LocalTransport()
         dist_mode = isinstance(self.transport, DistTransport)
         if dist_mode:

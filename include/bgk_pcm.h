@@ -216,10 +216,11 @@ int bgk_adjoint_run(bgk_ctx *ctx, const bgk_adjoint_spec *spec, double *loss,
  * 1 MiB per device. */
 #define BGK_STATIC_SUMS_MAX_NY 32768
 
-/* The four sums of bgk_field_sums (STEP_7/field_check.f90:9-17,
- * STEP_7/diag.f90:82-91) over fields the caller keeps in its own device
- * memory, computed without allocating anything.  No reference counterpart:
- * the reference sums its host arrays in place.
+/* The four sums of bgk_field_sums -- total density, total temperature,
+ * total liquid fraction and the number of liquid nodes (phi > 0) over the
+ * interior -- over fields the caller keeps in its own device memory,
+ * computed without allocating anything.  This entry point has no
+ * counterpart in the reference.
  *
  * For a caller that cannot allocate device memory mid-run: a host that owns
  * its rho/T/phi arrays on the GPU and must not create a context (bgk_create
@@ -242,8 +243,11 @@ int bgk_adjoint_run(bgk_ctx *ctx, const bgk_adjoint_spec *spec, double *loss,
  *  - Nothing in the scratch has to start at zero: every slot a call reads is
  *    written earlier by the same call.
  *  - The first call on each device looks up the scratch address
- *    (cudaGetSymbolAddress) and caches it; make that first call before any
- *    stream capture begins.
+ *    (cudaGetSymbolAddress) and caches it for the device's current CUDA
+ *    context; make that first call before any stream capture begins.  After
+ *    the context is replaced (cudaDeviceReset, or another context made
+ *    current), the next call repeats the lookup, and that call too belongs
+ *    outside a stream capture.
  *  - All calls on one device share the scratch.  Calls that can overlap in
  *    time (on different streams, or from host threads without ordering
  *    between them) race and return wrong sums; calls on one stream are

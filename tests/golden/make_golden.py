@@ -1,9 +1,10 @@
 #!/usr/bin/env python
 """Generate golden vectors by executing the reference's own STEP_7 source.
 
-Run where the reference sources are mounted (they are not needed afterwards):
+Run where the reference sources are mounted (they are not needed afterwards),
+giving the root of the reference checkout (the directory holding STEP_7/):
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference root>
 
 The STEP_7 routines (setup, initialization, BC_f, BC_g, streaming,
 momentsPre, phase_field, forces, collision, moments) are translated by
@@ -102,7 +103,12 @@ def run_case(ref: Path, params: dict, steps: int, order):
 
 
 def main():
-    ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    import argparse
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("reference", type=Path, help="root of the reference checkout (the directory holding STEP_7/)")
+    ref = ap.parse_args().reference
+    if not (ref / "STEP_7" / "main.f90").is_file():
+        ap.error(f"{ref}/STEP_7/main.f90 not found")
     order = main_loop_order(ref)
     assert order == ["bc_f", "bc_g", "streaming", "momentspre", "phase_field", "forces", "collision",
                      "moments"], order

@@ -268,3 +268,16 @@ def test_gloo_subgroup_addresses_peers_by_global_rank(oracle_mod):
     ref = _undivided(_params(), 7)
     assert res[0] is None and res[2] is None
     np.testing.assert_array_equal(res[1], ref["phi"])
+
+
+@pytest.mark.parametrize("wall", ["westBC", "eastBC", "northBC", "southBC"])
+def test_slab_run_rejects_walls_other_than_no_slip(wall):
+    """A slab builds inflow or pressure walls from its own rows, so only the
+    no-slip code 4 decomposes; SlabRun refuses anything else before it
+    creates a slab (even a call short enough to run only final chunks)."""
+    from bgk_pcm_b200.slab import SlabRun
+    params = dict(small_params(12, 16), **{wall: 2})
+    made = []
+    with pytest.raises(ValueError, match="code 4"):
+        SlabRun(params, nslabs=2, halo=2, slab_factory=lambda plan, r: made.append(r))
+    assert made == []

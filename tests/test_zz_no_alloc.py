@@ -88,3 +88,42 @@ def test_static_sums_match_context_sums(lib):
     cpu = torch.zeros(4, dtype=torch.float64)
     assert lib.bgk_field_sums_static(_ptr(dev["rho"]), _ptr(dev["T"]), _ptr(dev["phi"]), Nx, Ny, Nx + 2,
                                      ctypes.c_void_p(stream.cuda_stream), _ptr(cpu)) == -1
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not has_gpu(), reason="needs a GPU")
+def test_static_sums_at_the_row_limit_and_into_managed_memory(lib):
+    """The largest Ny the scratch holds, on a grid one column wide (ld = 3),
+    and a result buffer in managed memory (which the call accepts beside
+    device memory), both against numpy sums of the same fields."""
+    import torch
+    from bgk_pcm_b200 import capi
+    from cuda.bindings import runtime as rt
+
+    Nx, Ny = 1, capi.STATIC_SUMS_MAX_NY
+    rng = np.random.default_rng(7)
+    host = {"rho": 1.0 + 0.01 * rng.standard_normal((Ny + 2, Nx + 2)),
+            "T": 263.0 + 20.0 * rng.random((Ny + 2, Nx + 2)),
+            "phi": rng.uniform(-1.0, 1.0, (Ny + 2, Nx + 2))}
+    dev = {n: torch.from_numpy(a).to("cuda:0") for n, a in host.items()}
+    interior = {n: a[1:Ny + 1, 1:Nx + 1] for n, a in host.items()}
+    expect = np.array([interior["rho"].sum(), interior["T"].sum(), interior["phi"].sum(),
+                       float((interior["phi"] > 0).sum())])
+    stream = torch.cuda.current_stream("cuda:0")
+
+    err, mptr = rt.cudaMallocManaged(4 * 8, rt.cudaMemAttachGlobal)
+    assert err == rt.cudaError_t.cudaSuccess
+    try:
+        managed = np.ctypeslib.as_array((ctypes.c_double * 4).from_address(int(mptr)))
+        for _ in range(2):
+            managed[:] = np.nan
+            torch.cuda.synchronize()
+            rc = lib.bgk_field_sums_static(_ptr(dev["rho"]), _ptr(dev["T"]), _ptr(dev["phi"]), Nx, Ny, Nx + 2,
+                                           ctypes.c_void_p(stream.cuda_stream), ctypes.c_void_p(int(mptr)))
+            assert rc == 0, lib.bgk_last_error()
+            torch.cuda.synchronize()
+            got = managed.copy()
+            np.testing.assert_allclose(got, expect, rtol=RTOL, atol=1e-9)
+            assert got[3] == expect[3]
+    finally:
+        rt.cudaFree(mptr)
