@@ -320,6 +320,23 @@ def e2e_slab(params, precision, steps, halo, torch, dist, tanh="portable"):
     return ms, h2d, d2h
 
 
+def precision_errors(params, device) -> dict:
+    """Errors of the FP32 form against the FP64 path after the workload's
+    full run (params["iter"] steps), per field (max and RMS, normalised as
+    the target is stated: T by T0 - T_in_sol, phi by its range 2, u and v by
+    max |u| of the FP64 run) and for the melt front (x shift of phi's zero
+    crossing, at row Ny/2 and the largest over the rows).  The FP64 path is
+    the bit-exact one (the reference's roundings, portable tanh)."""
+    from bgk_pcm_b200 import precision as pr
+    steps = params["iter"]
+    t0 = time.perf_counter()
+    ref = pr.run(params, "f64", steps, tanh="portable")
+    lo = pr.run(params, "f32", steps)
+    e = pr.errors(lo, ref, params)
+    e.update({"steps": steps, "vs": "f64 (reference roundings, portable tanh)", "seconds": time.perf_counter() - t0})
+    return e
+
+
 def fp64_divergence(params, device, tanh_a, tanh_b, fma_b, steps=200) -> float:
     """Largest |difference| over rho, T, u, v, phi (halos included) between
     the headline FP64 form (tanh_a, exact operation order) and a variant
@@ -403,6 +420,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward cost leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--precision-errors", type=int, default=1,
+                    help="1: run the precision workload in full (FP64 and FP32) and report the FP32 form's errors")
     ap.add_argument("--decomp", default="slab", choices=["slab", "replicas"],
                     help="N > 1: y-slab decomposition of one N-times taller cavity, or N replicas")
     ap.add_argument("--halo", type=int, default=8, help="ghost rows per cut (steps between exchanges)")
@@ -521,6 +540,8 @@ def main():
                          "f32_over_f64": rates["f32"] / rates["f64"],
                          "f32_hbm_gbs": rates["f32"] * BYTES_PER_NODE["f32"],
                          "f32_frac_of_measured_hbm": rates["f32"] * BYTES_PER_NODE["f32"] / hbm}
+        if args.precision_errors:
+            precision_cfg["errors"] = precision_errors(pparams, local)
 
     adjoint = None
     if rank == 0 and world == 1 and not args.no_adjoint:

@@ -13,7 +13,11 @@
  *    (bounce-back, STEP_7/BC_f.f90:62-68,101-107,125-136,181-192) or of a
  *    per-row boundary array (STEP_7/BC_g.f90:7-31), except the two corner
  *    populations f6(Nx+1,0) and f7(Nx+1,Ny+1) that BC_f never writes; those
- *    two numbers are kept in `corner`.
+ *    two numbers are kept in `corner`.  With any other wall code the f halo
+ *    cells carry state of their own (periodic copies, inflow equilibria,
+ *    values that persist from step to step), so they are kept in a ring
+ *    (`fring`, see ring_idx) that a boundary kernel updates before each step
+ *    exactly as BC_f does, and the step pulls from it.
  *  - phi: compact interior plane, A/B ping-pong (its 3x3 stencil reads the
  *    previous step's values).  Columns 0 and Nx+1 are frozen boundary values
  *    (phiW/phiE per row); rows 0 and Ny+1 are copies of rows 1 and Ny.
@@ -74,10 +78,24 @@ struct StepPtrs {
     const double *pE;      /* [3][Ny]  east equilibrium polynomials k=3,6,7 */
     const double *phiW, *phiE;   /* [Ny]                                    */
     double *mrho, *mT, *mu, *mv, *mphi;  /* mirrors, or null               */
+    const double *ring;    /* f halo ring [9][ring_len] (walls other than 4) */
+    long long ring_len;
     long long plane;       /* elements per population plane                */
     int P;                 /* row pitch (elements)                          */
     int NX2;               /* mirror pitch                                   */
 };
+
+/* Offset of halo cell (i, j) of the reference's (0:Nx+1, 0:Ny+1) layout in
+ * one population's ring: column 0 (rows 0..Ny+1, corners included), column
+ * Nx+1 (rows 0..Ny+1), row 0 (columns 1..Nx), row Ny+1 (columns 1..Nx). */
+__host__ __device__ inline long long ring_idx(int Nx, int Ny, int i, int j)
+{
+    if (i == 0) return j;
+    if (i == Nx + 1) return (long long)(Ny + 2) + j;
+    if (j == 0) return 2LL * (Ny + 2) + (i - 1);
+    return 2LL * (Ny + 2) + Nx + (i - 1);
+}
+__host__ __device__ inline long long ring_length(int Nx, int Ny) { return 2LL * (Ny + 2) + 2LL * Nx; }
 
 struct LowpScale {
     float sf, sg;          /* FP16 form: stored = deviation * s            */
@@ -98,6 +116,8 @@ struct bgk_ctx {
     long long plane;       /* Ny*P                                          */
     size_t esz;            /* bytes per stored population element           */
     size_t phisz;          /* bytes per stored phi element (4 or 8)          */
+    int phi_pole;          /* 4-byte phi stored as its distance to the nearer
+                            * of -1 and +1 (reduced-precision forms)        */
     int it;
 
     /* fused state (each buffer has a 256-byte guard on both sides: the
@@ -126,6 +146,9 @@ struct bgk_ctx {
     double *scratch;       /* A doubles                                     */
     double *red;           /* reduction partials; red[0..3] = results        */
     double *corner;        /* f6(Nx+1,0), f7(Nx+1,Ny+1) (never written by BC_f) */
+    bool ring;             /* a wall other than code 4: f halos in fring     */
+    double *fring;         /* [9][ring_len] f halo cells (ring_idx), or null */
+    long long ring_len;
     int red_n;
     double *pinned;        /* small pinned host buffer                      */
 
@@ -146,6 +169,7 @@ namespace bgk {
 /* kernels_f64.cu (compiled with --fmad=false: the reference's roundings) */
 cudaError_t launch_init_f64(bgk_ctx *c);
 cudaError_t launch_bc_prep(bgk_ctx *c);
+cudaError_t launch_ring_bc(bgk_ctx *c);            /* BC_f + BC_g halos, walls other than 4 */
 cudaError_t launch_macro_halos(bgk_ctx *c);
 cudaError_t launch_fused_f64(bgk_ctx *c, bool moments);
 cudaError_t launch_staged(bgk_ctx *c, int stage);   /* 1..8 in main.f90 order */

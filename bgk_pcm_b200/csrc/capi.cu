@@ -417,13 +417,31 @@ int bgk_create(const bgk_params *pp, const bgk_options *opt, bgk_ctx **out)
     c->A = (size_t)c->NX2 * (size_t)c->NY2;
     c->P = (pp->Nx + 31) / 32 * 32;
     c->plane = (long long)c->P * pp->Ny;
+    if (const char *v = getenv("BGK_PLANE_PAD")) {
+        /* extra elements between consecutive population planes, a multiple
+         * of 32 so every row stays 128-byte aligned */
+        const long long pad = atoll(v);
+        if (pad > 0) c->plane += (pad + 31) / 32 * 32;
+    }
     c->esz = o.precision == BGK_PREC_F64 ? 8 : (o.precision == BGK_PREC_F16 ? 2 : 4);
-    /* phi: FP64 in the FP64 and FP32X forms; FP32 (storage and phase-field
-     * arithmetic) in the FP32 and FP16 forms unless BGK_LP_PHI64=1 */
+    /* phi: FP64 in the FP64 and FP32X forms; 32 bits (storage and
+     * phase-field arithmetic in FP32) in the FP32 and FP16 forms, either as
+     * the plain value ("float") or as the distance to the nearer pole
+     * ("pole"); BGK_LP_PHI = float | pole | f64 selects, BGK_LP_PHI64=1 is
+     * f64 */
     c->phisz = (o.precision == BGK_PREC_F64 || o.precision == BGK_PREC_F32X) ? 8 : 4;
+    c->phi_pole = 0;
     if (o.precision == BGK_PREC_F32 || o.precision == BGK_PREC_F16) {
         const char *v = getenv("BGK_LP_PHI64");
         if (v && atoi(v) == 1) c->phisz = 8;
+        if (const char *m = getenv("BGK_LP_PHI")) {
+            if (!strcmp(m, "f64")) c->phisz = 8;
+            else if (!strcmp(m, "pole")) c->phi_pole = 1;
+            else if (strcmp(m, "float")) {
+                delete c;
+                return fail(BGK_ERR_ARG, "BGK_LP_PHI must be float, pole or f64");
+            }
+        }
     }
     c->it = 0;
     c->cur = 0;
@@ -478,6 +496,14 @@ int bgk_create(const bgk_params *pp, const bgk_options *opt, bgk_ctx **out)
     c->red_n = 4 + 4 * 592;
     DA(c->red, (size_t)c->red_n * sizeof(double), "reduction");
     DA(c->corner, 2 * sizeof(double), "corners");
+    /* walls other than the no-slip code 4 (FP64 only): the f halo ring */
+    c->ring = o.precision == BGK_PREC_F64 && !all_bc4(*pp);
+    c->ring_len = bgk::ring_length(c->Nx, c->Ny);
+    c->fring = nullptr;
+    if (c->ring) {
+        DA(c->fring, (size_t)9 * (size_t)c->ring_len * sizeof(double), "f halo ring");
+        CK(cudaMemsetAsync(c->fring, 0, (size_t)9 * (size_t)c->ring_len * sizeof(double), c->stream), "memset");
+    }
     e = cudaMallocHost(&c->pinned, 64 * sizeof(double));
     if (e != cudaSuccess) { bgk_destroy(c); return cuda_fail(e, "cudaMallocHost"); }
     CK(cudaStreamSynchronize(c->stream), "create");
@@ -493,7 +519,7 @@ int bgk_destroy(bgk_ctx *c)
     void *ptrs[] = {c->raw[0], c->raw[1], c->raw[2], c->raw[3], c->raw[4], c->raw[5], c->errflag,
                     c->tcol[0], c->tcol[1], c->gW, c->pE, c->phiW, c->phiE, c->tin_rows,
                     c->mrho, c->mT, c->mu, c->mv, c->mphi, c->sphip, c->srho2, c->sT2, c->su2, c->sv2,
-                    c->scratch, c->red, c->corner};
+                    c->scratch, c->red, c->corner, c->fring};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (int k = 0; k < 9; k++) {
@@ -535,13 +561,12 @@ int bgk_step(bgk_ctx *c, int nsteps)
     if (!c) return fail(BGK_ERR_ARG, "null context");
     if (nsteps < 0) return fail(BGK_ERR_ARG, "nsteps < 0");
     if (nsteps == 0) return BGK_OK;
-    if (!all_bc4(c->p))
-        return fail(BGK_ERR_UNSUPPORTED, "the fused step implements the no-slip code 4 on every wall; "
-                                         "use the staged entry points for codes 0/1/2/3/5/6");
+    if (!all_bc4(c->p) && !c->ring)
+        return fail(BGK_ERR_UNSUPPORTED, "the reduced-precision forms implement the no-slip code 4 on every wall");
     int rc = set_device(c);
     if (rc) return rc;
     if ((rc = ensure_fused(c))) return rc;
-    if (c->bc_dirty) {
+    if (c->bc_dirty && !c->ring) {
         CK(bgk::launch_bc_prep(c), "bc_prep");
         c->bc_dirty = false;
     }
@@ -551,7 +576,14 @@ int bgk_step(bgk_ctx *c, int nsteps)
     for (int t = 0; t < nsteps; t++) {
         const bool last = (t == nsteps - 1);
         const bool mom = last || (t == nsteps - 2);
-        if (last) CK(bgk::launch_macro_halos(c), "macro_halos");
+        if (c->ring) {
+            /* BC_f and the halo part of BC_g every step, then the west/east
+             * g values from this step's velocity halos (STEP_7/BC_g.f90:7-31) */
+            CK(bgk::launch_ring_bc(c), "ring boundary");
+            CK(bgk::launch_bc_prep(c), "bc_prep");
+        } else if (last) {
+            CK(bgk::launch_macro_halos(c), "macro_halos");
+        }
         if (exact) CK(bgk::launch_fused_f64(c, mom), "fused step");
         else CK(bgk::launch_fused_fast(c, mom), "fused step");
         c->cur ^= 1;
@@ -790,7 +822,7 @@ int bgk_save(bgk_ctx *c, const char *path)
     if ((rc = ensure_fused(c))) return rc;
     FILE *fp = fopen(path, "wb");
     if (!fp) return fail(BGK_ERR_IO, "cannot write %s", path);
-    const int hdr[8] = {c->Nx, c->Ny, c->opt.precision, c->it, c->P, c->tin_host ? 1 : 0, 0, 0};
+    const int hdr[8] = {c->Nx, c->Ny, c->opt.precision, c->it, c->P, c->tin_host ? 1 : 0, c->ring ? 1 : 0, 0};
     bool ok = fwrite(kMagic, 1, 8, fp) == 8 && fwrite(hdr, sizeof hdr, 1, fp) == 1;
     const size_t popbytes = (size_t)9 * c->plane * c->esz;
     const size_t phibytes = (size_t)c->plane * c->phisz;
@@ -812,6 +844,7 @@ int bgk_save(bgk_ctx *c, const char *path)
     put(c->mu, c->A * sizeof(double));
     put(c->mv, c->A * sizeof(double));
     put(c->mphi, c->A * sizeof(double));
+    if (c->ring) put(c->fring, (size_t)9 * (size_t)c->ring_len * sizeof(double));
     if (ok && c->opt.precision == BGK_PREC_F16) ok = fwrite(&c->scale, sizeof c->scale, 1, fp) == 1;
     if (ok && c->tin_host) ok = fwrite(c->tin_host, sizeof(double), c->Ny, fp) == (size_t)c->Ny;
     if (fclose(fp) != 0) ok = false;
@@ -830,7 +863,8 @@ int bgk_load(bgk_ctx *c, const char *path)
     int hdr[8];
     bool ok = fread(mg, 1, 8, fp) == 8 && memcmp(mg, kMagic, 8) == 0 && fread(hdr, sizeof hdr, 1, fp) == 1;
     if (!ok) { fclose(fp); return fail(BGK_ERR_IO, "%s is not a snapshot", path); }
-    if (hdr[0] != c->Nx || hdr[1] != c->Ny || hdr[2] != c->opt.precision || hdr[4] != c->P) {
+    if (hdr[0] != c->Nx || hdr[1] != c->Ny || hdr[2] != c->opt.precision || hdr[4] != c->P ||
+        hdr[6] != (c->ring ? 1 : 0)) {
         fclose(fp);
         return fail(BGK_ERR_ARG, "snapshot is %dx%d precision %d; context is %dx%d precision %d", hdr[0], hdr[1],
                     hdr[2], c->Nx, c->Ny, c->opt.precision);
@@ -859,6 +893,7 @@ int bgk_load(bgk_ctx *c, const char *path)
     get(c->mu, c->A * sizeof(double));
     get(c->mv, c->A * sizeof(double));
     get(c->mphi, c->A * sizeof(double));
+    if (c->ring) get(c->fring, (size_t)9 * (size_t)c->ring_len * sizeof(double));
     if (ok && c->opt.precision == BGK_PREC_F16) ok = fread(&c->scale, sizeof c->scale, 1, fp) == 1;
     std::vector<double> tin;
     if (ok && hdr[5]) {

@@ -46,10 +46,10 @@ __device__ __forceinline__ void prefetch_row(const T *F, const T *G, const TP *P
  * forces, collision, stores and (when required) moments.  Shared by the
  * register-pull kernel below and the shared-memory pipeline kernel
  * (fused_pipe.cuh), so both round identically. */
-template <int TANH, bool MOM, bool REF32>
+template <int TANH, bool MOM, bool REF32, bool RING = false>
 __device__ __forceinline__ void node_f64(const StepPtrs<double> &s, const Consts &c, int x, int y, long long cc,
                                          bool E, double *f, double *g, const double (&ap)[3][3],
-                                         const double (&am)[3][3], const double *pc)
+                                         const double (&am)[3][3], const double *pc, bool edge = false)
 {
     const long long pl = s.plane;
     /* momentsPre */
@@ -87,11 +87,14 @@ __device__ __forceinline__ void node_f64(const StepPtrs<double> &s, const Consts
     for (int k = 0; k < 9; k++) s.gout[k * pl + cc] = out[k];
     s.phout[cc] = phn;
 
-    /* moments (all nodes on output steps; column Nx every step) */
-    if (MOM || E) {
+    /* moments (all nodes on output steps; column Nx every step; with a wall
+     * other than code 4, every edge node every step: the next step's BC_f
+     * reads rho, u and v there) */
+    const bool wm = MOM || (RING && edge);
+    if (wm || E) {
         const double Tm = (sum9(out) + T2) * 0.5;
         if (E) s.tcout[y] = Tm;
-        if (MOM) {
+        if (wm) {
             const double rm = sum9(f);
             const double irm = 1.0 / rm;
             const double tu = irm * xmom(f);

@@ -69,7 +69,7 @@ __device__ __forceinline__ void pipe_issue(const S *F, const S *G, const PT *PH,
     bulk_g2s(stage + 18 * Gm::POP_BYTES, PH + (long long)rp * P + x0 - Gm::ALP, Gm::PHI_BYTES, full);
 }
 
-template <int D, int TANH, bool MOM, bool REF32>
+template <int D, int TANH, bool MOM, bool REF32, bool RING = false>
 __global__ void __launch_bounds__(PIPE_THREADS, 3)
 fused_pipe_f64_kernel(StepPtrs<double> s, Consts c, const double *__restrict__ corner, PipeSched sch, int *errflag)
 {
@@ -178,7 +178,23 @@ fused_pipe_f64_kernel(StepPtrs<double> s, Consts c, const double *__restrict__ c
                 f[6] = sp[6 * Gm::RW + col + 1];
                 f[7] = sp[7 * Gm::RW + col + 1];
                 f[8] = sp[8 * Gm::RW + col - 1];
-                if (W || E || S || N) {
+                if (RING) {
+                    /* pulls from outside the domain read the halo ring,
+                     * which the boundary kernel filled as BC_f does */
+                    if (W || E || S || N) {
+                        const double *R = s.ring;
+                        const long long RL = s.ring_len;
+                        const int i = x + 1, j = y + 1;
+                        if (W) f[1] = R[1 * RL + ring_idx(Nx, Ny, 0, j)];
+                        if (S) f[2] = R[2 * RL + ring_idx(Nx, Ny, i, 0)];
+                        if (E) f[3] = R[3 * RL + ring_idx(Nx, Ny, Nx + 1, j)];
+                        if (N) f[4] = R[4 * RL + ring_idx(Nx, Ny, i, Ny + 1)];
+                        if (W || S) f[5] = R[5 * RL + ring_idx(Nx, Ny, i - 1, j - 1)];
+                        if (E || S) f[6] = R[6 * RL + ring_idx(Nx, Ny, i + 1, j - 1)];
+                        if (E || N) f[7] = R[7 * RL + ring_idx(Nx, Ny, i + 1, j + 1)];
+                        if (W || N) f[8] = R[8 * RL + ring_idx(Nx, Ny, i - 1, j + 1)];
+                    }
+                } else if (W || E || S || N) {
                     /* bounce-back values that are not in the stage */
                     if (S) f[2] = F[4 * pl + cc];
                     if (N) f[4] = F[2 * pl + cc];
@@ -209,7 +225,7 @@ fused_pipe_f64_kernel(StepPtrs<double> s, Consts c, const double *__restrict__ c
                     g[6] = sg[6 * Gm::RW + col + 1];
                     g[7] = sg[7 * Gm::RW + col + 1];
                 }
-                node_f64<TANH, MOM, REF32>(s, c, x, y, cc, E, f, g, ap, am, pc);
+                node_f64<TANH, MOM, REF32, RING>(s, c, x, y, cc, E, f, g, ap, am, pc, W || E || S || N);
 #pragma unroll
                 for (int k = 0; k < 3; k++) {
                     ap[0][k] = ap[1][k]; ap[1][k] = ap[2][k];
@@ -226,13 +242,13 @@ fused_pipe_f64_kernel(StepPtrs<double> s, Consts c, const double *__restrict__ c
     }
 }
 
-template <int D, int T, bool M, bool R>
+template <int D, int T, bool M, bool R, bool RING = false>
 inline cudaError_t pipe_f64_launch(const bgk_ctx *c, const StepPtrs<double> &s, int ctas)
 {
     using Gm = PipeGeom<double, double>;
     const size_t smem = Gm::smem_bytes(D);
     static std::atomic<unsigned long long> done{0};
-    const cudaError_t e = pipe_configure(fused_pipe_f64_kernel<D, T, M, R>, smem, c->dev, done);
+    const cudaError_t e = pipe_configure(fused_pipe_f64_kernel<D, T, M, R, RING>, smem, c->dev, done);
     if (e != cudaSuccess) return e;
     int grid;
     const PipeSched sch = pipe_sched(c, ctas, 4, &grid);
@@ -240,10 +256,28 @@ inline cudaError_t pipe_f64_launch(const bgk_ctx *c, const StepPtrs<double> &s, 
      * steps are short enough (tens of microseconds) for the launch gap to
      * matter: +9 % at 512^2; on larger grids it measured ~1 % slower */
     if ((long long)c->Nx * c->Ny <= (1LL << 21))
-        return pdl_launch(fused_pipe_f64_kernel<D, T, M, R>, grid, PIPE_THREADS, smem, c->stream, s, c->c,
+        return pdl_launch(fused_pipe_f64_kernel<D, T, M, R, RING>, grid, PIPE_THREADS, smem, c->stream, s, c->c,
                           (const double *)c->corner, sch, c->errflag);
-    fused_pipe_f64_kernel<D, T, M, R><<<grid, PIPE_THREADS, smem, c->stream>>>(s, c->c, c->corner, sch, c->errflag);
+    fused_pipe_f64_kernel<D, T, M, R, RING><<<grid, PIPE_THREADS, smem, c->stream>>>(s, c->c, c->corner, sch,
+                                                                                   c->errflag);
     return cudaGetLastError();
+}
+
+/* Walls other than code 4: two stages (the default depth), the halo ring. */
+inline cudaError_t pipe_f64_ring_dispatch(const bgk_ctx *c, const StepPtrs<double> &s, bool mom, int ctas)
+{
+    const bool portable = c->opt.tanh_mode == BGK_TANH_PORTABLE;
+    const bool ref32 = !c->opt.smooth;
+    if (portable) {
+        if (mom) return ref32 ? pipe_f64_launch<2, BGK_TANH_PORTABLE, true, true, true>(c, s, ctas)
+                              : pipe_f64_launch<2, BGK_TANH_PORTABLE, true, false, true>(c, s, ctas);
+        return ref32 ? pipe_f64_launch<2, BGK_TANH_PORTABLE, false, true, true>(c, s, ctas)
+                     : pipe_f64_launch<2, BGK_TANH_PORTABLE, false, false, true>(c, s, ctas);
+    }
+    if (mom) return ref32 ? pipe_f64_launch<2, BGK_TANH_DEVICE, true, true, true>(c, s, ctas)
+                          : pipe_f64_launch<2, BGK_TANH_DEVICE, true, false, true>(c, s, ctas);
+    return ref32 ? pipe_f64_launch<2, BGK_TANH_DEVICE, false, true, true>(c, s, ctas)
+                 : pipe_f64_launch<2, BGK_TANH_DEVICE, false, false, true>(c, s, ctas);
 }
 
 template <int D>
@@ -269,6 +303,7 @@ inline cudaError_t pipe_f64_dispatch(const bgk_ctx *c, const StepPtrs<double> &s
  * slots. */
 inline cudaError_t launch_fused_pipe_f64(const bgk_ctx *c, const StepPtrs<double> &s, bool mom)
 {
+    if (c->ring) return pipe_f64_ring_dispatch(c, s, mom, c->tune_ctas > 0 ? c->tune_ctas : 3);
     const int D = c->tune_D > 0 ? c->tune_D : 2;
     const int ctas = c->tune_ctas > 0 ? c->tune_ctas : (D <= 2 ? 3 : 2);
     switch (D) {

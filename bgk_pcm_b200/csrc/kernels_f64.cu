@@ -42,7 +42,8 @@ struct Staged {
  * the compact populations (interior) or the staged arrays, and phi twice
  * (phi and phi_prec are equal after initialization). */
 __global__ void init_kernel(Consts c, int westBC, StepPtrs<double> s, double *fcomp, double *gcomp,
-                            double *phc0, double *phc1, Staged st, bool staged, double *corner, double *tcol)
+                            double *phc0, double *phc1, Staged st, bool staged, double *corner, double *tcol,
+                            double *ring, long long RL)
 {
     const int NX2 = c.Nx + 2, NY2 = c.Ny + 2;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -90,6 +91,8 @@ __global__ void init_kernel(Consts c, int westBC, StepPtrs<double> s, double *fc
     if (i == Nx + 1 && j == 0) corner[0] = fe[6];
     if (i == Nx + 1 && j == Ny + 1) corner[1] = fe[7];
     if (i == Nx && j >= 1 && j <= Ny) tcol[j - 1] = T;
+    if (ring && (i == 0 || i == Nx + 1 || j == 0 || j == Ny + 1))
+        for (int k = 0; k < 9; k++) ring[k * RL + ring_idx(Nx, Ny, i, j)] = fe[k];
 }
 
 /* ------------------------------------------------------- boundary prep */
@@ -116,6 +119,29 @@ __global__ void bc_prep_kernel(Consts c, const double *mu, const double *mv, con
     pE[2 * Ny + j - 1] = P[7];
     phiW[j - 1] = mphi[qw];
     phiE[j - 1] = mphi[qe];
+}
+
+/* Halo cells between population rings and reference-layout arrays (pitch
+ * Nx+2): block row y copies population k0 + y to or from refs.p[y]
+ * (to_ring: ref -> ring, else ring -> ref). */
+struct Ptr9 {
+    double *p[9];
+};
+
+__global__ void ring_ref_copy(int Nx, int Ny, double *ring, long long RL, Ptr9 refs, int k0, bool to_ring)
+{
+    const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (r >= RL) return;
+    const int k = k0 + blockIdx.y;
+    int i, j;
+    if (r < Ny + 2) { i = 0; j = (int)r; }
+    else if (r < 2LL * (Ny + 2)) { i = Nx + 1; j = (int)(r - (Ny + 2)); }
+    else if (r < 2LL * (Ny + 2) + Nx) { i = (int)(r - 2LL * (Ny + 2)) + 1; j = 0; }
+    else { i = (int)(r - 2LL * (Ny + 2) - Nx) + 1; j = Ny + 1; }
+    double *ref = refs.p[blockIdx.y];
+    const size_t q = (size_t)i + (size_t)(Nx + 2) * (size_t)j;
+    if (to_ring) ring[k * RL + r] = ref[q];
+    else ref[q] = ring[k * RL + r];
 }
 
 /* ------------------------------------------------------ macroscopic halos */
@@ -320,6 +346,179 @@ __global__ void staged_bc_g(Staged s, Consts c)
         for (int k = 0; k < 9; k++) s.g[k][SQ(i, 0)] = s.g[k][SQ(i, 1)];
         s.T[SQ(i, 0)] = s.T[SQ(i, 1)];
         s.phi[SQ(i, 0)] = s.phi[SQ(i, 1)];
+    }
+}
+
+/* --------------------------------------------- ring boundary (codes != 4) */
+
+/* BC_f (STEP_7/BC_f.f90:5-200, every branch, west, east, north, south in that
+ * order) on the fused state: interior f from the compact planes of the
+ * current buffer, halo f in the ring, rho/u/v in the mirrors (which hold the
+ * previous step's moments on the edge rows and columns and the reference's
+ * halo values).  Then the macroscopic halo assignments of BC_g
+ * (STEP_7/BC_g.f90:7-64): T west/east, then T and phi north/south.  One
+ * block; the phases are separated by barriers, so each reads what the
+ * previous ones wrote, as in the reference.  The g halos themselves are not
+ * stored: the step computes them (west and east from bc_prep's per-row
+ * values, north and south as copies). */
+struct RingF {
+    const double *fc;      /* compact planes (current buffer) */
+    double *ring;
+    long long plane, RL;
+    int P, Nx, Ny;
+    __device__ double get(int k, int i, int j) const
+    {
+        if (i >= 1 && i <= Nx && j >= 1 && j <= Ny) return fc[k * plane + (long long)(j - 1) * P + (i - 1)];
+        return ring[k * RL + ring_idx(Nx, Ny, i, j)];
+    }
+    __device__ void set(int k, int i, int j, double v) const { ring[k * RL + ring_idx(Nx, Ny, i, j)] = v; }
+};
+
+__global__ void ring_bc_kernel(Consts c, RingF F, double *rho, double *u, double *v, double *T, double *phi,
+                               const double *tin, const double *tcol, int wbc, int ebc, int nbc, int sbc)
+{
+    const int Nx = c.Nx, Ny = c.Ny, NX2 = Nx + 2;
+    const double *w = c.w;
+    const int t0 = threadIdx.x, nt = blockDim.x;
+    double P[9];
+    /* WEST */
+    if (wbc == 0) {
+        for (int j = t0; j <= Ny + 1; j += nt)
+            for (int k = 0; k < 9; k++) F.set(k, 0, j, F.get(k, Nx, j));
+    } else if (wbc == 1) {
+        eq_poly(c.u0, c.v0, P);
+        for (int j = 1 + t0; j <= Ny; j += nt) {
+            double r = rho[SQ(1, j)];
+            F.set(1, 0, j, w[1] * r * P[1]);
+            F.set(5, 0, j, w[5] * r * P[5]);
+            F.set(8, 0, j, w[8] * r * P[8]);
+            u[SQ(0, j)] = c.u0;
+            v[SQ(0, j)] = c.v0;
+            rho[SQ(0, j)] = rho[SQ(1, j)];
+        }
+    } else if (wbc == 2) {
+        for (int j = t0; j <= Ny + 1; j += nt) {
+            eq_poly(u[SQ(0, j)], c.v0, P);
+            double r = rho[SQ(1, j)];
+            F.set(1, 0, j, w[1] * r * P[1]);
+            F.set(5, 0, j, w[5] * r * P[5]);
+            F.set(8, 0, j, w[8] * r * P[8]);
+        }
+    } else if (wbc == 3) {
+        for (int j = t0; j <= Ny + 1; j += nt) {
+            double u1 = u[SQ(1, j)], v1 = v[SQ(1, j)];
+            eq_poly(u1, v1, P);
+            F.set(1, 0, j, w[1] * c.rho1 * P[1]);
+            F.set(5, 0, j, w[5] * c.rho1 * P[5]);
+            F.set(8, 0, j, w[8] * c.rho1 * P[8]);
+            u[SQ(0, j)] = u1;
+            v[SQ(0, j)] = v1;
+            rho[SQ(0, j)] = c.rho1;
+        }
+    } else if (wbc == 4) {
+        for (int j = 1 + t0; j <= Ny; j += nt) {
+            F.set(1, 0, j, F.get(3, 1, j));
+            F.set(8, 0, j, F.get(6, 1, j - 1));
+            F.set(5, 0, j, F.get(7, 1, j + 1));
+        }
+    }
+    __syncthreads();
+    /* EAST */
+    if (ebc == 0) {
+        for (int j = t0; j <= Ny + 1; j += nt)
+            for (int k = 0; k < 9; k++) F.set(k, Nx + 1, j, F.get(k, 1, j));
+    } else if (ebc == 3) {
+        for (int j = 1 + t0; j <= Ny; j += nt) {
+            double un = u[SQ(Nx, j)], vn = v[SQ(Nx, j)];
+            eq_poly(un, vn, P);
+            F.set(3, Nx + 1, j, w[3] * c.rho0 * P[3]);
+            F.set(6, Nx + 1, j, w[6] * c.rho0 * P[6]);
+            F.set(7, Nx + 1, j, w[7] * c.rho0 * P[7]);
+            u[SQ(Nx + 1, j)] = un;
+            v[SQ(Nx + 1, j)] = vn;
+            rho[SQ(Nx + 1, j)] = c.rho0;
+        }
+    } else if (ebc == 4) {
+        for (int j = 1 + t0; j <= Ny; j += nt) {
+            F.set(3, Nx + 1, j, F.get(1, Nx, j));
+            F.set(6, Nx + 1, j, F.get(8, Nx, j + 1));
+            F.set(7, Nx + 1, j, F.get(5, Nx, j - 1));
+        }
+    }
+    __syncthreads();
+    /* NORTH */
+    if (nbc == 0) {
+        for (int i = t0; i <= Nx + 1; i += nt)
+            for (int k = 0; k < 9; k++) F.set(k, i, Ny + 1, F.get(k, i, 1));
+    } else if (nbc == 4) {
+        for (int i = 1 + t0; i <= Nx; i += nt) {
+            F.set(4, i, Ny + 1, F.get(2, i, Ny));
+            F.set(7, i, Ny + 1, F.get(5, i - 1, Ny));
+            F.set(8, i, Ny + 1, F.get(6, i + 1, Ny));
+            rho[SQ(i, Ny + 1)] = rho[SQ(i, Ny)];
+            u[SQ(i, Ny + 1)] = 0.0;
+            v[SQ(i, Ny + 1)] = 0.0;
+        }
+        if (t0 == 0) F.set(8, 0, Ny + 1, F.get(6, 1, Ny));
+    } else if (nbc == 5) {
+        for (int i = t0; i <= Nx + 1; i += nt) {
+            F.set(4, i, Ny + 1, F.get(2, i, Ny - 1));
+            F.set(7, i, Ny + 1, F.get(6, i, Ny - 1));
+            F.set(8, i, Ny + 1, F.get(5, i, Ny - 1));
+        }
+    } else if (nbc == 6) {
+        for (int i = t0; i <= Nx + 1; i += nt) {
+            F.set(4, i, Ny + 1, F.get(4, i, Ny));
+            F.set(7, i, Ny + 1, F.get(7, i, Ny));
+            F.set(8, i, Ny + 1, F.get(8, i, Ny));
+        }
+    } else if (nbc == 1) {
+        eq_poly(c.u0, c.v0, P);
+        for (int i = t0; i <= Nx + 1; i += nt) {
+            double r = rho[SQ(i, Ny)];
+            F.set(4, i, Ny + 1, w[4] * r * P[4]);
+            F.set(7, i, Ny + 1, w[7] * r * P[7]);
+            F.set(8, i, Ny + 1, w[8] * r * P[8]);
+        }
+    }
+    __syncthreads();
+    /* SOUTH */
+    if (sbc == 0) {
+        for (int i = t0; i <= Nx + 1; i += nt)
+            for (int k = 0; k < 9; k++) F.set(k, i, 0, F.get(k, i, Ny));
+    } else if (sbc == 4) {
+        for (int i = 1 + t0; i <= Nx; i += nt) {
+            F.set(2, i, 0, F.get(4, i, 1));
+            F.set(5, i, 0, F.get(7, i + 1, 1));
+            F.set(6, i, 0, F.get(8, i - 1, 1));
+            rho[SQ(i, 0)] = rho[SQ(i, 1)];
+            u[SQ(i, 0)] = 0.0;
+            v[SQ(i, 0)] = 0.0;
+        }
+        if (t0 == 0) F.set(5, 0, 0, F.get(7, 1, 1));
+    } else if (sbc == 6) {
+        for (int i = t0; i <= Nx + 1; i += nt) {
+            F.set(2, i, 0, F.get(2, i, 1));
+            F.set(5, i, 0, F.get(5, i, 1));
+            F.set(6, i, 0, F.get(6, i, 1));
+        }
+    }
+    __syncthreads();
+    /* BC_g, macroscopic part: T west/east (T(Nx,j) of the previous moments
+     * is tcol), then T and phi north/south */
+    for (int j = 1 + t0; j <= Ny; j += nt) {
+        T[SQ(0, j)] = tin ? tin[j - 1] : c.Tin;
+        T[SQ(Nx + 1, j)] = tcol[j - 1];
+    }
+    __syncthreads();
+    for (int i = t0; i <= Nx + 1; i += nt) {
+        T[SQ(i, Ny + 1)] = T[SQ(i, Ny)];
+        phi[SQ(i, Ny + 1)] = phi[SQ(i, Ny)];
+    }
+    __syncthreads();
+    for (int i = t0; i <= Nx + 1; i += nt) {
+        T[SQ(i, 0)] = T[SQ(i, 1)];
+        phi[SQ(i, 0)] = phi[SQ(i, 1)];
     }
 }
 
@@ -576,7 +775,23 @@ cudaError_t launch_init_f64(bgk_ctx *c)
         staged ? nullptr : (double *)c->fbuf[c->cur],
         staged ? nullptr : (double *)c->gbuf[c->cur],
         (double *)c->phibuf[0], (double *)c->phibuf[1], staged_of(c), staged,
-        c->corner, c->tcol[c->cur]);
+        c->corner, c->tcol[c->cur], (!staged && c->ring) ? c->fring : nullptr, c->ring_len);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ring_bc(bgk_ctx *c)
+{
+    RingF F;
+    F.fc = (const double *)c->fbuf[c->cur];
+    F.ring = c->fring;
+    F.plane = c->plane;
+    F.RL = c->ring_len;
+    F.P = c->P;
+    F.Nx = c->Nx;
+    F.Ny = c->Ny;
+    ring_bc_kernel<<<1, 1024, 0, c->stream>>>(c->c, F, c->mrho, c->mu, c->mv, c->mT, c->mphi, c->tin_rows,
+                                               c->tcol[c->cur], c->p.westBC, c->p.eastBC, c->p.northBC,
+                                               c->p.southBC);
     return cudaGetLastError();
 }
 
@@ -615,11 +830,11 @@ cudaError_t launch_fused_f64(bgk_ctx *c, bool moments)
     s.gW = c->gW; s.pE = c->pE; s.phiW = c->phiW; s.phiE = c->phiE;
     s.mrho = c->mrho; s.mT = c->mT; s.mu = c->mu; s.mv = c->mv; s.mphi = c->mphi;
     s.plane = c->plane; s.P = c->P; s.NX2 = c->NX2;
+    s.ring = c->fring; s.ring_len = c->ring_len;
     const int H = strip_height(c);
     dim3 grd((c->Nx + FUSED_BX - 1) / FUSED_BX, (c->Ny + H - 1) / H);
-    const double *corner = corner_ptr(c);
-    (void)corner;
-    if (c->tune_pipe) return launch_fused_pipe_f64(c, s, moments);
+    /* walls other than code 4 run on the pipeline kernel only */
+    if (c->tune_pipe || c->ring) return launch_fused_pipe_f64(c, s, moments);
     return launch_fused_f64_variant(c, grd, s, H, moments);
 }
 
@@ -668,12 +883,33 @@ cudaError_t launch_staged(bgk_ctx *c, int stage)
     return cudaGetLastError();
 }
 
+/* the f halo cells between the ring and the staged arrays */
+static cudaError_t ring_staged(bgk_ctx *c, bool to_ring)
+{
+    Ptr9 refs;
+    for (int k = 0; k < 9; k++) refs.p[k] = c->sf[k];
+    dim3 grd((unsigned)((c->ring_len + 255) / 256), 9);
+    ring_ref_copy<<<grd, 256, 0, c->stream>>>(c->Nx, c->Ny, c->fring, c->ring_len, refs, 0, to_ring);
+    return cudaGetLastError();
+}
+
+/* the f halo cells of population k between the ring and a reference-layout field */
+static cudaError_t ring_field(bgk_ctx *c, int k, double *ref, bool to_ring)
+{
+    Ptr9 refs{};
+    refs.p[0] = ref;
+    dim3 grd((unsigned)((c->ring_len + 255) / 256), 1);
+    ring_ref_copy<<<grd, 256, 0, c->stream>>>(c->Nx, c->Ny, c->fring, c->ring_len, refs, k, to_ring);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_compact_to_staged(bgk_ctx *c)
 {
     Staged s = staged_of(c);
     dim3 blk(64, 4);
     compact_to_staged_kernel<<<interior_grid(c, blk), blk, 0, c->stream>>>(
         s, c->c, (const double *)c->fbuf[c->cur], (const double *)c->gbuf[c->cur], c->plane, c->P, corner_ptr(c));
+    if (c->ring) return ring_staged(c, false);
     return cudaGetLastError();
 }
 
@@ -684,6 +920,7 @@ cudaError_t launch_staged_to_compact(bgk_ctx *c)
     staged_to_compact_kernel<<<interior_grid(c, blk), blk, 0, c->stream>>>(
         s, c->c, (double *)c->fbuf[c->cur], (double *)c->gbuf[c->cur], (double *)c->phibuf[c->cur],
         (double *)c->phibuf[c->cur ^ 1], c->plane, c->P, corner_ptr(c), c->tcol[c->cur]);
+    if (c->ring) return ring_staged(c, true);
     return cudaGetLastError();
 }
 
@@ -695,6 +932,10 @@ cudaError_t launch_ref_to_compact(bgk_ctx *c, int field, const double *ref)
     if (field >= BGK_FIELD_F0 && field < BGK_FIELD_F0 + 9) {
         const int k = field - BGK_FIELD_F0;
         ref_to_plane_kernel<<<grd, blk, 0, c->stream>>>(c->c, ref, (double *)c->fbuf[c->cur] + k * c->plane, c->P);
+        if (c->ring) {
+            cudaError_t e = ring_field(c, k, const_cast<double *>(ref), true);
+            if (e != cudaSuccess) return e;
+        }
         if (k == 6 || k == 7) {
             const size_t q = (k == 6) ? (size_t)(c->Nx + 1) : (size_t)(c->Nx + 1) + (size_t)c->NX2 * (size_t)(c->Ny + 1);
             cudaError_t e = cudaMemcpyAsync(corner_ptr(c) + (k - 6), ref + q, sizeof(double),
@@ -724,6 +965,8 @@ cudaError_t launch_compact_to_ref(bgk_ctx *c, int field, double *ref, int which)
         const double *cn = (k == 6) ? corner_ptr(c) : (k == 7 ? corner_ptr(c) + 1 : nullptr);
         plane_to_ref_kernel<<<grd, blk, 0, c->stream>>>(c->c, (const double *)c->fbuf[b] + k * c->plane, c->P, ref,
                                                          nullptr, c->Nx + 1, k == 6 ? 0 : c->Ny + 1, cn);
+        /* the ring holds the halo of the current step only */
+        if (c->ring && !which) return ring_field(c, k, ref, false);
     } else if (field >= BGK_FIELD_G0 && field < BGK_FIELD_G0 + 9) {
         const int k = field - BGK_FIELD_G0;
         plane_to_ref_kernel<<<grd, blk, 0, c->stream>>>(c->c, (const double *)c->gbuf[b] + k * c->plane, c->P, ref,

@@ -49,9 +49,10 @@ cudaError_t launch_fused_fast(bgk_ctx *c, bool moments)
     s.gW = c->gW; s.pE = c->pE; s.phiW = c->phiW; s.phiE = c->phiE;
     s.mrho = c->mrho; s.mT = c->mT; s.mu = c->mu; s.mv = c->mv; s.mphi = c->mphi;
     s.plane = c->plane; s.P = c->P; s.NX2 = c->NX2;
+    s.ring = c->fring; s.ring_len = c->ring_len;
     const int H = strip_height(c);
     dim3 grd((c->Nx + FUSED_BX - 1) / FUSED_BX, (c->Ny + H - 1) / H);
-    if (c->tune_pipe) return launch_fused_pipe_f64(c, s, moments);
+    if (c->tune_pipe || c->ring) return launch_fused_pipe_f64(c, s, moments);
     return launch_fused_f64_variant(c, grd, s, H, moments);
 }
 
@@ -102,11 +103,6 @@ template <> struct Codec<float> {
     static __device__ __forceinline__ float ld(const float *p, float) { return __ldg(p); }
     static __device__ __forceinline__ float lds(const float *p, float) { return *p; }
     static __device__ __forceinline__ void st(float *p, float v, float) { *p = v; }
-};
-template <> struct Codec<double> {
-    static __device__ __forceinline__ float ld(const double *p, float) { return (float)__ldg(p); }
-    static __device__ __forceinline__ float lds(const double *p, float) { return (float)*p; }
-    static __device__ __forceinline__ void st(double *p, float v, float) { *p = (double)v; }
 };
 template <> struct Codec<__half> {
     static __device__ __forceinline__ float ld(const __half *p, float inv) { return __half2float(__ldg(p)) * inv; }
@@ -191,6 +187,69 @@ __device__ __forceinline__ double tanh_pt<double>(double x, int mode)
     return mode == BGK_TANH_PORTABLE ? bgk_portable_tanh(x) : tanh(x);
 }
 
+/* Phase-field storage.  The update of STEP_7/phase_field.f90:22-48 needs,
+ * per cell, the two bases 1 + phi and 1 - phi (of the selector terms
+ * (1/2 (1 +- phi))^2 and of the update itself).  A codec gives both for a
+ * stored word, phi in double, and the encoding of an updated value.
+ *
+ * float / double: phi itself.  In FP32 a cell near a pole (phi ~ -1 in the
+ * solid, +1 in the liquid) has an ulp of 6e-8, so per-step updates smaller
+ * than 3e-8 -- the slow growth of the liquid fraction ahead of the melt
+ * front -- round away, and the front lags the FP64 run.
+ * PhiQ: 32 bits holding the distance to the nearer pole, signed by the pole:
+ * q = -(1 + phi) for phi <= 0 (sign bit set, -0 at phi = -1), q = 1 - phi
+ * for phi > 0.  Whichever of 1 +- phi is small is then held to full float
+ * precision, and an update of any size changes it. */
+struct PhiQ {
+    float q;
+};
+
+template <typename PS> struct PhiCodec;
+template <> struct PhiCodec<float> {
+    using A = float;
+    static __device__ __forceinline__ float onep(float s) { return 1.f + s; }
+    static __device__ __forceinline__ float onem(float s) { return 1.f - s; }
+    static __device__ __forceinline__ double dec(float s) { return (double)s; }
+    static __device__ __forceinline__ float from_d(double phi) { return (float)phi; }
+    static __device__ __forceinline__ float update(float s, float kpp, float kmm)
+    {
+        return s + (0.5f * kpp * (1.f - s) - 0.5f * kmm * (1.f + s));
+    }
+};
+template <> struct PhiCodec<double> {
+    using A = double;
+    static __device__ __forceinline__ double onep(double s) { return 1.0 + s; }
+    static __device__ __forceinline__ double onem(double s) { return 1.0 - s; }
+    static __device__ __forceinline__ double dec(double s) { return s; }
+    static __device__ __forceinline__ double from_d(double phi) { return phi; }
+    static __device__ __forceinline__ double update(double s, double kpp, double kmm)
+    {
+        return s + (0.5 * kpp * (1.0 - s) - 0.5 * kmm * (1.0 + s));
+    }
+};
+template <> struct PhiCodec<PhiQ> {
+    using A = float;
+    static __device__ __forceinline__ float onep(PhiQ s) { return signbit(s.q) ? -s.q : 2.f - s.q; }
+    static __device__ __forceinline__ float onem(PhiQ s) { return signbit(s.q) ? 2.f + s.q : s.q; }
+    static __device__ __forceinline__ double dec(PhiQ s)
+    {
+        return signbit(s.q) ? -1.0 - (double)s.q : 1.0 - (double)s.q;
+    }
+    static __device__ __forceinline__ PhiQ from_d(double phi)
+    {
+        return phi <= 0.0 ? PhiQ{-(float)fabs(1.0 + phi)} : PhiQ{(float)fabs(1.0 - phi)};
+    }
+    /* new phi = phi + d, d = kpp (1 - phi)/2 - kmm (1 + phi)/2, carried on
+     * the small base; a base that rounding takes below zero is a pole */
+    static __device__ __forceinline__ PhiQ update(PhiQ s, float kpp, float kmm)
+    {
+        const float op = onep(s), om = onem(s);
+        const float d = 0.5f * kpp * om - 0.5f * kmm * op;
+        const float opn = op + d, omn = om - d;
+        return opn <= omn ? PhiQ{-fabsf(opn)} : PhiQ{fabsf(omn)};
+    }
+};
+
 /* One node of a reduced-precision step after its pulls (deviations in AT):
  * momentsPre, phase field (PT), latent heat (FP64), forces, collision,
  * stores, moments.  Shared by the register-pull and pipeline kernels.
@@ -209,8 +268,11 @@ __device__ __forceinline__ double tanh_pt<double>(double x, int mode)
  * mass and energy up to the rounding of f_0 and g_0 themselves. */
 template <typename S, typename PT, typename AT, int TANH, bool MOM>
 __device__ __forceinline__ void node_lp(const LpPtrs<S, PT> &s, const ConstsLP<AT> &c, int x, int y, long long cc,
-                                        bool E, AT *f, AT *g, PT kp, PT km, PT p0)
+                                        bool E, AT *f, AT *g, typename PhiCodec<PT>::A kp,
+                                        typename PhiCodec<PT>::A km, PT q0)
 {
+    using PC = PhiCodec<PT>;
+    using PA = typename PC::A;
     using C = Codec<S>;
     const long long pl = s.plane;
     /* momentsPre (deviations; the energy in FP64) */
@@ -225,16 +287,17 @@ __device__ __forceinline__ void node_lp(const LpPtrs<S, PT> &s, const ConstsLP<A
     AT v = irho * (f[2] - f[4] + f[5] + f[6] - f[7] - f[8]);
     const AT dT2 = dT, u2 = u, v2 = v;
 
-    /* phase_field (in PT) */
-    const PT one = (PT)1, half = (PT)0.5;
-    const PT th = tanh_pt<PT>(((PT)c.T0mTcrit_d + (PT)dT) * (PT)c.inv_T_width_d, TANH);
-    const PT kpp = kp * (PT)0.125 * (half * (one + th));
-    const PT kmm = km * (PT)0.125 * (half * (one - th));
-    const PT phn_p = p0 + (half * kpp * (one - p0) - half * kmm * (one + p0));
-    const AT phn = (AT)phn_p;
+    /* phase_field (in PA) */
+    const PA one = (PA)1, half = (PA)0.5;
+    const PA th = tanh_pt<PA>(((PA)c.T0mTcrit_d + (PA)dT) * (PA)c.inv_T_width_d, TANH);
+    const PA kpp = kp * (PA)0.125 * (half * (one + th));
+    const PA kmm = km * (PA)0.125 * (half * (one - th));
+    const PT qn = PC::update(q0, kpp, kmm);
+    const double p0d = PC::dec(q0), pnd = PC::dec(qn);
+    const AT phn = (AT)pnd;
 
-    /* forces: latent heat in FP64 */
-    dTd -= c.dts * ((double)phn_p - (double)p0) * 0.5;
+    /* forces: latent heat in FP64, on the change of the stored phi */
+    dTd -= c.dts * (pnd - p0d) * 0.5;
     dT = (AT)dTd;
     const AT T = c.T0 + dT;
     const AT omp = (AT)1 - phn;
@@ -271,7 +334,7 @@ __device__ __forceinline__ void node_lp(const LpPtrs<S, PT> &s, const ConstsLP<A
     }
 #pragma unroll
     for (int k = 0; k < 9; k++) C::st(s.gout + k * pl + cc, (float)out[k], s.sg);
-    s.phout[cc] = phn_p;
+    s.phout[cc] = qn;
 
     if (MOM || E) {
         AT sg = 0;
@@ -292,7 +355,7 @@ __device__ __forceinline__ void node_lp(const LpPtrs<S, PT> &s, const ConstsLP<A
             s.mT[q] = Tm;
             s.mu[q] = 0.5 * ((double)tu + (double)u2);
             s.mv[q] = 0.5 * ((double)tv + (double)v2);
-            s.mphi[q] = (double)phn_p;
+            s.mphi[q] = pnd;
         }
     }
 }
@@ -314,16 +377,19 @@ fused_lowp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, int H, int pf)
     const PT *__restrict__ PH = s.phin;
     const float isf = s.inv_sf, isg = s.inv_sg;
 
-    PT ap[3], am[3], pc[3];   /* per row y-1, y, y+1: sums over x-1..x+1 of (1/2 (1 +- phi))^2, and phi */
+    using PC = PhiCodec<PT>;
+    using PA = typename PC::A;
+    PA ap[3], am[3];   /* per row y-1, y, y+1: sums over x-1..x+1 of (1/2 (1 +- phi))^2 */
+    PT pc[3];          /* and the stored phi of column x */
     auto load_row = [&](int r, int slot) {
         const int rc = r < 0 ? 0 : (r >= Ny ? Ny - 1 : r);
         const PT *row = PH + (long long)rc * P;
-        const PT pL = W ? (PT)s.phiW[rc] : row[x - 1];
+        const PT pL = W ? PC::from_d(s.phiW[rc]) : row[x - 1];
         const PT pM = row[x];
-        const PT pR = E ? (PT)s.phiE[rc] : row[x + 1];
-        const PT h = (PT)0.5, one = (PT)1;
-        const PT a0 = h * (one + pL), a1 = h * (one + pM), a2 = h * (one + pR);
-        const PT b0 = h * (one - pL), b1 = h * (one - pM), b2 = h * (one - pR);
+        const PT pR = E ? PC::from_d(s.phiE[rc]) : row[x + 1];
+        const PA h = (PA)0.5;
+        const PA a0 = h * PC::onep(pL), a1 = h * PC::onep(pM), a2 = h * PC::onep(pR);
+        const PA b0 = h * PC::onem(pL), b1 = h * PC::onem(pM), b2 = h * PC::onem(pR);
         ap[slot] = a0 * a0 + a1 * a1 + a2 * a2;
         am[slot] = b0 * b0 + b1 * b1 + b2 * b2;
         pc[slot] = pM;
@@ -428,6 +494,8 @@ fused_pipe_lp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, PipeSched sch, int *errfla
         pdl_allow_next();
         return;
     }
+    using PC = PhiCodec<PT>;
+    using PA = typename PC::A;
     const long long pl = s.plane;
     const int P = s.P;
     const S *__restrict__ F = s.fin;
@@ -440,18 +508,19 @@ fused_pipe_lp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, PipeSched sch, int *errfla
         const int x = it.x0 + tid;
         const bool active = x < Nx;
         const bool W = (x == 0), E = (x == Nx - 1);
-        PT ap[3], am[3], pc[3];   /* per row y-1, y, y+1: sums over x-1..x+1 of (1/2 (1 +- phi))^2, and phi */
-        const PT h = (PT)0.5, one = (PT)1;
+        PA ap[3], am[3];   /* per row y-1, y, y+1: sums over x-1..x+1 of (1/2 (1 +- phi))^2 */
+        PT pc[3];          /* and the stored phi of column x */
+        const PA h = (PA)0.5;
         if (active) {
             for (int slot = 0; slot < 2; slot++) {
                 const int rr = it.y - 1 + slot;
                 const int rc = rr < 0 ? 0 : (rr >= Ny ? Ny - 1 : rr);
                 const PT *row = PH + (long long)rc * P;
-                const PT pL = W ? (PT)s.phiW[rc] : row[x - 1];
+                const PT pL = W ? PC::from_d(s.phiW[rc]) : row[x - 1];
                 const PT pM = row[x];
-                const PT pR = E ? (PT)s.phiE[rc] : row[x + 1];
-                const PT a0 = h * (one + pL), a1 = h * (one + pM), a2 = h * (one + pR);
-                const PT b0 = h * (one - pL), b1 = h * (one - pM), b2 = h * (one - pR);
+                const PT pR = E ? PC::from_d(s.phiE[rc]) : row[x + 1];
+                const PA a0 = h * PC::onep(pL), a1 = h * PC::onep(pM), a2 = h * PC::onep(pR);
+                const PA b0 = h * PC::onem(pL), b1 = h * PC::onem(pM), b2 = h * PC::onem(pR);
                 ap[slot] = a0 * a0 + a1 * a1 + a2 * a2;
                 am[slot] = b0 * b0 + b1 * b1 + b2 * b2;
                 pc[slot] = pM;
@@ -476,11 +545,11 @@ fused_pipe_lp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, PipeSched sch, int *errfla
                 const int col = tid + Gm::AL;
                 {
                     const int rc = (y + 1 >= Ny) ? Ny - 1 : y + 1;
-                    const PT pL = W ? (PT)s.phiW[rc] : sphi[Gm::ALP + tid - 1];
+                    const PT pL = W ? PC::from_d(s.phiW[rc]) : sphi[Gm::ALP + tid - 1];
                     const PT pM = sphi[Gm::ALP + tid];
-                    const PT pR = E ? (PT)s.phiE[rc] : sphi[Gm::ALP + tid + 1];
-                    const PT a0 = h * (one + pL), a1 = h * (one + pM), a2 = h * (one + pR);
-                    const PT b0 = h * (one - pL), b1 = h * (one - pM), b2 = h * (one - pR);
+                    const PT pR = E ? PC::from_d(s.phiE[rc]) : sphi[Gm::ALP + tid + 1];
+                    const PA a0 = h * PC::onep(pL), a1 = h * PC::onep(pM), a2 = h * PC::onep(pR);
+                    const PA b0 = h * PC::onem(pL), b1 = h * PC::onem(pM), b2 = h * PC::onem(pR);
                     ap[2] = a0 * a0 + a1 * a1 + a2 * a2;
                     am[2] = b0 * b0 + b1 * b1 + b2 * b2;
                     pc[2] = pM;
@@ -585,7 +654,7 @@ __global__ void init_lowp_kernel(Consts c, S *fd, S *gd, PT *ph0, PT *ph1, long 
         Codec<S>::st(fd + k * plane + cc, (float)(c.w[k] * rho * Pq[k] - c.w[k] * c.rho0), sf);
         Codec<S>::st(gd + k * plane + cc, (float)(c.w[k] * T * Pq[k] - c.w[k] * c.T0), sg);
     }
-    const PT phi = (i <= c.interf) ? (PT)1 : (PT)-1;
+    const PT phi = PhiCodec<PT>::from_d((i <= c.interf) ? 1.0 : -1.0);
     ph0[cc] = phi;
     ph1[cc] = phi;
 }
@@ -615,6 +684,29 @@ __global__ void lp_plane_to_ref(Consts c, const S *src, int P, double *ref, doub
         ref[q] = halo_src[q];
     else
         ref[q] = (corner && i == ci && j == cj) ? corner[0] : 0.0;
+}
+
+/* reference-layout phi <-> a stored phi plane (any phi codec) */
+template <typename PT>
+__global__ void phi_ref_to_plane(Consts c, const double *ref, PT *dst, int P)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= c.Nx || y >= c.Ny) return;
+    dst[(long long)y * P + x] = PhiCodec<PT>::from_d(ref[(size_t)(x + 1) + (size_t)(c.Nx + 2) * (size_t)(y + 1)]);
+}
+
+template <typename PT>
+__global__ void phi_plane_to_ref(Consts c, const PT *src, int P, double *ref, const double *halo_src)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > c.Nx + 1 || j > c.Ny + 1) return;
+    const size_t q = (size_t)i + (size_t)(c.Nx + 2) * (size_t)j;
+    if (i >= 1 && i <= c.Nx && j >= 1 && j <= c.Ny)
+        ref[q] = PhiCodec<PT>::dec(src[(long long)(j - 1) * P + (i - 1)]);
+    else
+        ref[q] = halo_src[q];
 }
 
 __global__ void lp_tcol_kernel(Consts c, const double *ref, double *tcol)
@@ -703,9 +795,12 @@ cudaError_t launch_fused_lowp(bgk_ctx *c, bool moments)
 {
     const bool p64 = c->phisz == 8;
     if (c->opt.precision == BGK_PREC_F32X) return launch_lowp_t<float, double, double>(c, moments);
-    if (c->opt.precision == BGK_PREC_F32)
-        return p64 ? launch_lowp_t<float, double, float>(c, moments) : launch_lowp_t<float, float, float>(c, moments);
-    return p64 ? launch_lowp_t<__half, double, float>(c, moments) : launch_lowp_t<__half, float, float>(c, moments);
+    if (c->opt.precision == BGK_PREC_F32) {
+        if (p64) return launch_lowp_t<float, double, float>(c, moments);
+        return c->phi_pole ? launch_lowp_t<float, PhiQ, float>(c, moments) : launch_lowp_t<float, float, float>(c, moments);
+    }
+    if (p64) return launch_lowp_t<__half, double, float>(c, moments);
+    return c->phi_pole ? launch_lowp_t<__half, PhiQ, float>(c, moments) : launch_lowp_t<__half, float, float>(c, moments);
 }
 
 /* FP16 scales: powers of two that put the largest deviations expected in
@@ -744,9 +839,12 @@ cudaError_t launch_init_lowp(bgk_ctx *c)
     init_lowp_kernel<S, PT><<<grd, blk, 0, c->stream>>>(c->c, (S *)fb, (S *)gb, (PT *)c->phibuf[0],     \
                                                         (PT *)c->phibuf[1], c->plane, c->P, sf_, sg_)
     if (c->opt.precision != BGK_PREC_F16) {
-        if (p64) BGK_INIT(float, double, 1.f, 1.f); else BGK_INIT(float, float, 1.f, 1.f);
+        if (p64) BGK_INIT(float, double, 1.f, 1.f);
+        else if (c->phi_pole) BGK_INIT(float, PhiQ, 1.f, 1.f);
+        else BGK_INIT(float, float, 1.f, 1.f);
     } else {
         if (p64) BGK_INIT(__half, double, c->scale.sf, c->scale.sg);
+        else if (c->phi_pole) BGK_INIT(__half, PhiQ, c->scale.sf, c->scale.sg);
         else BGK_INIT(__half, float, c->scale.sf, c->scale.sg);
     }
 #undef BGK_INIT
@@ -771,12 +869,13 @@ static int lp_to_compact(bgk_ctx *c, int field, const double *ref)
         lp_ref_to_plane<S><<<grd, blk, 0, c->stream>>>(c->c, ref, (S *)c->gbuf[c->cur] + k * c->plane, c->P,
                                                        c->c.w[k] * c->c.T0, c->scale.sg);
     } else if (field == BGK_FIELD_PHI) {
-        if (c->phisz == 8) {
-            lp_ref_to_plane<double><<<grd, blk, 0, c->stream>>>(c->c, ref, (double *)c->phibuf[0], c->P, 0.0, 1.f);
-            lp_ref_to_plane<double><<<grd, blk, 0, c->stream>>>(c->c, ref, (double *)c->phibuf[1], c->P, 0.0, 1.f);
-        } else {
-            lp_ref_to_plane<float><<<grd, blk, 0, c->stream>>>(c->c, ref, (float *)c->phibuf[0], c->P, 0.0, 1.f);
-            lp_ref_to_plane<float><<<grd, blk, 0, c->stream>>>(c->c, ref, (float *)c->phibuf[1], c->P, 0.0, 1.f);
+        for (int b = 0; b < 2; b++) {
+            if (c->phisz == 8)
+                phi_ref_to_plane<double><<<grd, blk, 0, c->stream>>>(c->c, ref, (double *)c->phibuf[b], c->P);
+            else if (c->phi_pole)
+                phi_ref_to_plane<PhiQ><<<grd, blk, 0, c->stream>>>(c->c, ref, (PhiQ *)c->phibuf[b], c->P);
+            else
+                phi_ref_to_plane<float><<<grd, blk, 0, c->stream>>>(c->c, ref, (float *)c->phibuf[b], c->P);
         }
     } else if (field == BGK_FIELD_T) {
         lp_tcol_kernel<<<(c->Ny + 127) / 128, 128, 0, c->stream>>>(c->c, ref, c->tcol[c->cur]);
@@ -803,11 +902,11 @@ static int lp_to_ref(bgk_ctx *c, int field, double *ref, int prev)
                                                        c->c.w[k] * c->c.T0, c->scale.inv_sg, nullptr, -1, -1, nullptr);
     } else if (field == BGK_FIELD_PHI_PREC) {
         if (c->phisz == 8)
-            lp_plane_to_ref<double><<<grd, blk, 0, c->stream>>>(c->c, (const double *)c->phibuf[b], c->P, ref, 0.0,
-                                                                1.f, c->mphi, -1, -1, nullptr);
+            phi_plane_to_ref<double><<<grd, blk, 0, c->stream>>>(c->c, (const double *)c->phibuf[b], c->P, ref, c->mphi);
+        else if (c->phi_pole)
+            phi_plane_to_ref<PhiQ><<<grd, blk, 0, c->stream>>>(c->c, (const PhiQ *)c->phibuf[b], c->P, ref, c->mphi);
         else
-            lp_plane_to_ref<float><<<grd, blk, 0, c->stream>>>(c->c, (const float *)c->phibuf[b], c->P, ref, 0.0, 1.f,
-                                                               c->mphi, -1, -1, nullptr);
+            phi_plane_to_ref<float><<<grd, blk, 0, c->stream>>>(c->c, (const float *)c->phibuf[b], c->P, ref, c->mphi);
     } else {
         return BGK_ERR_UNSUPPORTED;
     }

@@ -42,8 +42,8 @@ def front_x(phi: np.ndarray) -> np.ndarray:
     return out
 
 
-def run(params: dict, precision: str, steps: int, smooth: bool = False) -> dict:
-    s = Solver(params, precision=precision, smooth=smooth)
+def run(params: dict, precision: str, steps: int, smooth: bool = False, tanh: str = "device") -> dict:
+    s = Solver(params, precision=precision, smooth=smooth, tanh=tanh)
     try:
         s.initialization()
         s.step(steps)

@@ -19,12 +19,18 @@
  *   correction so that k*head is exact), e^r - 1 by its Taylor series to
  *   degree 13, evaluated in Horner form.  Coefficients are 1/n! rounded to
  *   nearest double (computed with exact rational arithmetic).
+ *   The reduction and the Horner steps are explicit fused multiply-adds
+ *   (C99 fma, IEEE-754 fusedMultiplyAdd: one rounding), which both the host
+ *   libm and the GPU evaluate exactly as specified, so they stay
+ *   bit-identical even where the surrounding code forbids contraction; on
+ *   the GPU this halves the function's floating-point operations.
  * Accuracy: a few ulp over the whole real line (checked against libm by the
  * CPU test-suite).  This is a checking aid, not a replacement for tanh.
  */
 #ifndef BGK_PORTABLE_TANH_H
 #define BGK_PORTABLE_TANH_H
 
+#include <math.h>
 #include <stdint.h>
 #include <string.h>
 
@@ -55,26 +61,26 @@ BGK_PT_HD double bgk_pt_expm1_neg(double y)
     const double ln2_lo  = -0x1.718432a1b0e26p-35; /* ln 2 - ln2_hi     */
     /* e^-40 < 2^-57: below this, e^y - 1 rounds to -1 exactly */
     if (y < -40.0) return -1.0;
-    double kd = y * inv_ln2 + 0.5;
+    double kd = fma(y, inv_ln2, 0.5);
     /* floor without libm: truncate toward zero, fix negative non-integers */
     double t = (double)(long long)kd;
     if (t > kd) t = t - 1.0;
     int k = (int)t;
-    double r = (y - t * ln2_hi) - t * ln2_lo;
+    double r = fma(-t, ln2_lo, fma(-t, ln2_hi, y));
     /* e^r - 1 = r(1 + r/2 + r^2/6 + ... + r^12/13!) */
     double p = 0x1.6124613a86d09p-33;              /* 1/13! */
-    p = p * r + 0x1.1eed8eff8d898p-29;             /* 1/12! */
-    p = p * r + 0x1.ae64567f544e4p-26;             /* 1/11! */
-    p = p * r + 0x1.27e4fb7789f5cp-22;             /* 1/10! */
-    p = p * r + 0x1.71de3a556c734p-19;             /* 1/9!  */
-    p = p * r + 0x1.a01a01a01a01ap-16;             /* 1/8!  */
-    p = p * r + 0x1.a01a01a01a01ap-13;             /* 1/7!  */
-    p = p * r + 0x1.6c16c16c16c17p-10;             /* 1/6!  */
-    p = p * r + 0x1.1111111111111p-7;              /* 1/5!  */
-    p = p * r + 0x1.5555555555555p-5;              /* 1/4!  */
-    p = p * r + 0x1.5555555555555p-3;              /* 1/3!  */
-    p = p * r + 0.5;                               /* 1/2!  */
-    p = p * r + 1.0;                               /* 1/1!  */
+    p = fma(p, r, 0x1.1eed8eff8d898p-29);          /* 1/12! */
+    p = fma(p, r, 0x1.ae64567f544e4p-26);          /* 1/11! */
+    p = fma(p, r, 0x1.27e4fb7789f5cp-22);          /* 1/10! */
+    p = fma(p, r, 0x1.71de3a556c734p-19);          /* 1/9!  */
+    p = fma(p, r, 0x1.a01a01a01a01ap-16);          /* 1/8!  */
+    p = fma(p, r, 0x1.a01a01a01a01ap-13);          /* 1/7!  */
+    p = fma(p, r, 0x1.6c16c16c16c17p-10);          /* 1/6!  */
+    p = fma(p, r, 0x1.1111111111111p-7);           /* 1/5!  */
+    p = fma(p, r, 0x1.5555555555555p-5);           /* 1/4!  */
+    p = fma(p, r, 0x1.5555555555555p-3);           /* 1/3!  */
+    p = fma(p, r, 0.5);                            /* 1/2!  */
+    p = fma(p, r, 1.0);                            /* 1/1!  */
     double em = p * r;                             /* e^r - 1 */
     if (k == 0) return em;
     double s = bgk_pt_pow2i(k);
