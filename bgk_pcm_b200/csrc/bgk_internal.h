@@ -116,8 +116,6 @@ struct bgk_ctx {
     long long plane;       /* Ny*P                                          */
     size_t esz;            /* bytes per stored population element           */
     size_t phisz;          /* bytes per stored phi element (4 or 8)          */
-    int phi_pole;          /* 4-byte phi stored as its distance to the nearer
-                            * of -1 and +1 (reduced-precision forms)        */
     int it;
 
     /* fused state (each buffer has a 256-byte guard on both sides: the
@@ -160,6 +158,10 @@ struct bgk_ctx {
      * pulls; pipeline depth and CTAs per SM (BGK_PIPE, BGK_PIPE_D,
      * BGK_PIPE_CTAS) */
     int tune_pipe, tune_D, tune_ctas, nsm;
+    int tune_flow;         /* 1: reduced-precision steps between outputs in one
+                            * dataflow launch (BGK_FLOW)                    */
+    void *flow_buf;        /* its ticket counter and per-tile step counts   */
+    size_t flow_bytes;
     void *adj_ws;          /* adjoint workspace kept between bgk_adjoint_run calls */
     size_t adj_ws_bytes;
 };
@@ -172,6 +174,7 @@ cudaError_t launch_bc_prep(bgk_ctx *c);
 cudaError_t launch_ring_bc(bgk_ctx *c);            /* BC_f + BC_g halos, walls other than 4 */
 cudaError_t launch_macro_halos(bgk_ctx *c);
 cudaError_t launch_fused_f64(bgk_ctx *c, bool moments);
+cudaError_t launch_flow_f64(bgk_ctx *c, int nsteps);     /* dataflow steps, no moments */
 cudaError_t launch_staged(bgk_ctx *c, int stage);   /* 1..8 in main.f90 order */
 cudaError_t launch_compact_to_staged(bgk_ctx *c);
 cudaError_t launch_staged_to_compact(bgk_ctx *c);
@@ -186,6 +189,8 @@ cudaError_t launch_fused_f64_ptrs(bgk_ctx *c, const double *fin, const double *g
 /* kernels_fast.cu (FMA allowed): FP64-FMA, FP32 and FP16 forms */
 cudaError_t launch_fused_fast(bgk_ctx *c, bool moments);
 cudaError_t launch_init_lowp(bgk_ctx *c);
+cudaError_t launch_flow_lowp(bgk_ctx *c, int nsteps);   /* dataflow steps, no moments */
+cudaError_t launch_flow_fast(bgk_ctx *c, int nsteps);   /* FMA FP64 or reduced precision */
 
 } // namespace bgk
 

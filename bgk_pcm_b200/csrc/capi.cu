@@ -417,31 +417,13 @@ int bgk_create(const bgk_params *pp, const bgk_options *opt, bgk_ctx **out)
     c->A = (size_t)c->NX2 * (size_t)c->NY2;
     c->P = (pp->Nx + 31) / 32 * 32;
     c->plane = (long long)c->P * pp->Ny;
-    if (const char *v = getenv("BGK_PLANE_PAD")) {
-        /* extra elements between consecutive population planes, a multiple
-         * of 32 so every row stays 128-byte aligned */
-        const long long pad = atoll(v);
-        if (pad > 0) c->plane += (pad + 31) / 32 * 32;
-    }
     c->esz = o.precision == BGK_PREC_F64 ? 8 : (o.precision == BGK_PREC_F16 ? 2 : 4);
-    /* phi: FP64 in the FP64 and FP32X forms; 32 bits (storage and
-     * phase-field arithmetic in FP32) in the FP32 and FP16 forms, either as
-     * the plain value ("float") or as the distance to the nearer pole
-     * ("pole"); BGK_LP_PHI = float | pole | f64 selects, BGK_LP_PHI64=1 is
-     * f64 */
+    /* phi: FP64 in the FP64 and FP32X forms; FP32 (storage and phase-field
+     * arithmetic) in the FP32 and FP16 forms unless BGK_LP_PHI64=1 */
     c->phisz = (o.precision == BGK_PREC_F64 || o.precision == BGK_PREC_F32X) ? 8 : 4;
-    c->phi_pole = 0;
     if (o.precision == BGK_PREC_F32 || o.precision == BGK_PREC_F16) {
         const char *v = getenv("BGK_LP_PHI64");
         if (v && atoi(v) == 1) c->phisz = 8;
-        if (const char *m = getenv("BGK_LP_PHI")) {
-            if (!strcmp(m, "f64")) c->phisz = 8;
-            else if (!strcmp(m, "pole")) c->phi_pole = 1;
-            else if (strcmp(m, "float")) {
-                delete c;
-                return fail(BGK_ERR_ARG, "BGK_LP_PHI must be float, pole or f64");
-            }
-        }
     }
     c->it = 0;
     c->cur = 0;
@@ -456,6 +438,8 @@ int bgk_create(const bgk_params *pp, const bgk_options *opt, bgk_ctx **out)
     if (const char *v = getenv("BGK_PIPE")) c->tune_pipe = atoi(v);
     if (const char *v = getenv("BGK_PIPE_D")) c->tune_D = atoi(v);
     if (const char *v = getenv("BGK_PIPE_CTAS")) c->tune_ctas = atoi(v);
+    c->tune_flow = 0;
+    if (const char *v = getenv("BGK_FLOW")) c->tune_flow = atoi(v);
     {
         cudaDeviceProp pr;
         c->nsm = (cudaGetDeviceProperties(&pr, dev) == cudaSuccess) ? pr.multiProcessorCount : 148;
@@ -519,7 +503,7 @@ int bgk_destroy(bgk_ctx *c)
     void *ptrs[] = {c->raw[0], c->raw[1], c->raw[2], c->raw[3], c->raw[4], c->raw[5], c->errflag,
                     c->tcol[0], c->tcol[1], c->gW, c->pE, c->phiW, c->phiE, c->tin_rows,
                     c->mrho, c->mT, c->mu, c->mv, c->mphi, c->sphip, c->srho2, c->sT2, c->su2, c->sv2,
-                    c->scratch, c->red, c->corner, c->fring};
+                    c->scratch, c->red, c->corner, c->fring, c->flow_buf};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (int k = 0; k < 9; k++) {
@@ -573,7 +557,16 @@ int bgk_step(bgk_ctx *c, int nsteps)
     c->pristine = false;
     const bool f64 = c->opt.precision == BGK_PREC_F64;
     const bool exact = f64 && !c->opt.fma;
-    for (int t = 0; t < nsteps; t++) {
+    int t = 0;
+    if (c->tune_flow && !c->ring && nsteps > 2) {
+        /* the steps before the two that write the moments, in one launch */
+        if (exact) CK(bgk::launch_flow_f64(c, nsteps - 2), "dataflow steps");
+        else CK(bgk::launch_flow_fast(c, nsteps - 2), "dataflow steps");
+        c->cur ^= (nsteps - 2) & 1;
+        c->it += nsteps - 2;
+        t = nsteps - 2;
+    }
+    for (; t < nsteps; t++) {
         const bool last = (t == nsteps - 1);
         const bool mom = last || (t == nsteps - 2);
         if (c->ring) {

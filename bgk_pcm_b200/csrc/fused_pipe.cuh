@@ -69,6 +69,122 @@ __device__ __forceinline__ void pipe_issue(const S *F, const S *G, const PT *PH,
     bulk_g2s(stage + 18 * Gm::POP_BYTES, PH + (long long)rp * P + x0 - Gm::ALP, Gm::PHI_BYTES, full);
 }
 
+/* Pipeline consumers of the FP64 step, shared by the per-step kernel and
+ * the multi-step (dataflow) kernel.
+ *
+ * f64_window_start: the selector terms of the phase-field window's first
+ * two rows (y0-1, y0) for column x, from global memory. */
+__device__ __forceinline__ void f64_window_start(const StepPtrs<double> &s, int Ny, int x, int y0, bool W, bool E,
+                                                 double (&ap)[3][3], double (&am)[3][3], double *pc)
+{
+    for (int slot = 0; slot < 2; slot++) {
+        const int rr = y0 - 1 + slot;
+        const int rc = rr < 0 ? 0 : (rr >= Ny ? Ny - 1 : rr);
+        const double *row = s.phin + (long long)rc * s.P;
+        const double pL = W ? s.phiW[rc] : row[x - 1];
+        const double pM = row[x];
+        const double pR = E ? s.phiE[rc] : row[x + 1];
+        ap[slot][0] = aplus(pL); ap[slot][1] = aplus(pM); ap[slot][2] = aplus(pR);
+        am[slot][0] = aminus(pL); am[slot][1] = aminus(pM); am[slot][2] = aminus(pR);
+        pc[slot] = pM;
+    }
+}
+
+/* f64_row: node (x, y) from a filled stage -- the window's new row y+1,
+ * the pulls (bounce-back, or the halo ring with other wall codes, and the
+ * g boundary values), node_f64, and the window shift. */
+template <int TANH, bool MOM, bool REF32, bool RING>
+__device__ __forceinline__ void f64_row(const StepPtrs<double> &s, const Consts &c, const double *__restrict__ corner,
+                                        const unsigned char *stage, int x, int y, int tid, bool W, bool E,
+                                        double (&ap)[3][3], double (&am)[3][3], double *pc)
+{
+    using Gm = PipeGeom<double, double>;
+    const int Nx = c.Nx, Ny = c.Ny;
+    const long long pl = s.plane;
+    const double *__restrict__ F = s.fin;
+    const double *stg = reinterpret_cast<const double *>(stage);
+    const double *sp = stg;                                    /* f planes */
+    const double *sg = stg + 9 * Gm::RW;                       /* g planes */
+    const double *sphi = stg + 18 * Gm::RW;
+    const bool S = (y == 0), N = (y == Ny - 1);
+    const long long cc = (long long)y * s.P + x;
+    const int col = tid + Gm::AL;
+    /* new phi row y+1 of the window */
+    {
+        const int rc = (y + 1 >= Ny) ? Ny - 1 : y + 1;
+        const double pL = W ? s.phiW[rc] : sphi[Gm::ALP + tid - 1];
+        const double pM = sphi[Gm::ALP + tid];
+        const double pR = E ? s.phiE[rc] : sphi[Gm::ALP + tid + 1];
+        ap[2][0] = aplus(pL); ap[2][1] = aplus(pM); ap[2][2] = aplus(pR);
+        am[2][0] = aminus(pL); am[2][1] = aminus(pM); am[2][2] = aminus(pR);
+        pc[2] = pM;
+    }
+    double f[9], g[9];
+    f[0] = sp[0 * Gm::RW + col];
+    f[1] = W ? sp[3 * Gm::RW + col] : sp[1 * Gm::RW + col - 1];
+    f[2] = sp[2 * Gm::RW + col];
+    f[3] = E ? sp[1 * Gm::RW + col] : sp[3 * Gm::RW + col + 1];
+    f[4] = sp[4 * Gm::RW + col];
+    f[5] = sp[5 * Gm::RW + col - 1];
+    f[6] = sp[6 * Gm::RW + col + 1];
+    f[7] = sp[7 * Gm::RW + col + 1];
+    f[8] = sp[8 * Gm::RW + col - 1];
+    if (RING) {
+        /* pulls from outside the domain read the halo ring, which the
+         * boundary kernel filled as BC_f does */
+        if (W || E || S || N) {
+            const double *R = s.ring;
+            const long long RL = s.ring_len;
+            const int i = x + 1, j = y + 1;
+            if (W) f[1] = R[1 * RL + ring_idx(Nx, Ny, 0, j)];
+            if (S) f[2] = R[2 * RL + ring_idx(Nx, Ny, i, 0)];
+            if (E) f[3] = R[3 * RL + ring_idx(Nx, Ny, Nx + 1, j)];
+            if (N) f[4] = R[4 * RL + ring_idx(Nx, Ny, i, Ny + 1)];
+            if (W || S) f[5] = R[5 * RL + ring_idx(Nx, Ny, i - 1, j - 1)];
+            if (E || S) f[6] = R[6 * RL + ring_idx(Nx, Ny, i + 1, j - 1)];
+            if (E || N) f[7] = R[7 * RL + ring_idx(Nx, Ny, i + 1, j + 1)];
+            if (W || N) f[8] = R[8 * RL + ring_idx(Nx, Ny, i - 1, j + 1)];
+        }
+    } else if (W || E || S || N) {
+        /* bounce-back values that are not in the stage */
+        if (S) f[2] = F[4 * pl + cc];
+        if (N) f[4] = F[2 * pl + cc];
+        if (W || S) f[5] = F[7 * pl + cc];
+        if (E || S) f[6] = (E && S) ? corner[0] : F[8 * pl + cc];
+        if (E || N) f[7] = (E && N) ? corner[1] : F[5 * pl + cc];
+        if (W || N) f[8] = F[6 * pl + cc];
+    }
+    const int ym = S ? y : y - 1, yp = N ? y : y + 1;
+    g[0] = sg[0 * Gm::RW + col];
+    g[2] = sg[2 * Gm::RW + col];
+    g[4] = sg[4 * Gm::RW + col];
+    if (W) {
+        g[1] = s.gW[y];
+        g[5] = s.gW[Ny + ym];
+        g[8] = s.gW[2 * Ny + yp];
+    } else {
+        g[1] = sg[1 * Gm::RW + col - 1];
+        g[5] = sg[5 * Gm::RW + col - 1];
+        g[8] = sg[8 * Gm::RW + col - 1];
+    }
+    if (E) {
+        g[3] = c.w[3] * s.tcin[y] * s.pE[y];
+        g[6] = c.w[6] * s.tcin[ym] * s.pE[Ny + ym];
+        g[7] = c.w[7] * s.tcin[yp] * s.pE[2 * Ny + yp];
+    } else {
+        g[3] = sg[3 * Gm::RW + col + 1];
+        g[6] = sg[6 * Gm::RW + col + 1];
+        g[7] = sg[7 * Gm::RW + col + 1];
+    }
+    node_f64<TANH, MOM, REF32, RING>(s, c, x, y, cc, E, f, g, ap, am, pc, W || E || S || N);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        ap[0][k] = ap[1][k]; ap[1][k] = ap[2][k];
+        am[0][k] = am[1][k]; am[1][k] = am[2][k];
+    }
+    pc[0] = pc[1]; pc[1] = pc[2];
+}
+
 template <int D, int TANH, bool MOM, bool REF32, bool RING = false>
 __global__ void __launch_bounds__(PIPE_THREADS, 3)
 fused_pipe_f64_kernel(StepPtrs<double> s, Consts c, const double *__restrict__ corner, PipeSched sch, int *errflag)
@@ -115,10 +231,6 @@ fused_pipe_f64_kernel(StepPtrs<double> s, Consts c, const double *__restrict__ c
     }
 
     /* ---------------- consumers ---------------- */
-    const long long pl = s.plane;
-    const int P = s.P;
-    const double *__restrict__ F = s.fin;
-    const double *__restrict__ PH = s.phin;
     PipeIter it;
     long long r = 0;
     bool ok = it.start(sch, Ny);
@@ -127,19 +239,7 @@ fused_pipe_f64_kernel(StepPtrs<double> s, Consts c, const double *__restrict__ c
         const bool active = x < Nx;
         const bool W = (x == 0), E = (x == Nx - 1);
         double ap[3][3], am[3][3], pc[3];
-        if (active) {
-            for (int slot = 0; slot < 2; slot++) {
-                const int rr = it.y - 1 + slot;
-                const int rc = rr < 0 ? 0 : (rr >= Ny ? Ny - 1 : rr);
-                const double *row = PH + (long long)rc * P;
-                const double pL = W ? s.phiW[rc] : row[x - 1];
-                const double pM = row[x];
-                const double pR = E ? s.phiE[rc] : row[x + 1];
-                ap[slot][0] = aplus(pL); ap[slot][1] = aplus(pM); ap[slot][2] = aplus(pR);
-                am[slot][0] = aminus(pL); am[slot][1] = aminus(pM); am[slot][2] = aminus(pR);
-                pc[slot] = pM;
-            }
-        }
+        if (active) f64_window_start(s, Ny, x, it.y, W, E, ap, am, pc);
         const int tile = it.t;
         bool failed = false;
         do {
@@ -150,89 +250,9 @@ fused_pipe_f64_kernel(StepPtrs<double> s, Consts c, const double *__restrict__ c
                 failed = true;
                 break;
             }
-            const double *stg = reinterpret_cast<const double *>(stages + (size_t)st * Gm::STAGE_BYTES);
-            const double *sp = stg;                                    /* f planes */
-            const double *sg = stg + 9 * Gm::RW;                       /* g planes */
-            const double *sphi = stg + 18 * Gm::RW;
-            if (active) {
-                const bool S = (y == 0), N = (y == Ny - 1);
-                const long long cc = (long long)y * P + x;
-                const int col = tid + Gm::AL;
-                /* new phi row y+1 of the window */
-                {
-                    const int rc = (y + 1 >= Ny) ? Ny - 1 : y + 1;
-                    const double pL = W ? s.phiW[rc] : sphi[Gm::ALP + tid - 1];
-                    const double pM = sphi[Gm::ALP + tid];
-                    const double pR = E ? s.phiE[rc] : sphi[Gm::ALP + tid + 1];
-                    ap[2][0] = aplus(pL); ap[2][1] = aplus(pM); ap[2][2] = aplus(pR);
-                    am[2][0] = aminus(pL); am[2][1] = aminus(pM); am[2][2] = aminus(pR);
-                    pc[2] = pM;
-                }
-                double f[9], g[9];
-                f[0] = sp[0 * Gm::RW + col];
-                f[1] = W ? sp[3 * Gm::RW + col] : sp[1 * Gm::RW + col - 1];
-                f[2] = sp[2 * Gm::RW + col];
-                f[3] = E ? sp[1 * Gm::RW + col] : sp[3 * Gm::RW + col + 1];
-                f[4] = sp[4 * Gm::RW + col];
-                f[5] = sp[5 * Gm::RW + col - 1];
-                f[6] = sp[6 * Gm::RW + col + 1];
-                f[7] = sp[7 * Gm::RW + col + 1];
-                f[8] = sp[8 * Gm::RW + col - 1];
-                if (RING) {
-                    /* pulls from outside the domain read the halo ring,
-                     * which the boundary kernel filled as BC_f does */
-                    if (W || E || S || N) {
-                        const double *R = s.ring;
-                        const long long RL = s.ring_len;
-                        const int i = x + 1, j = y + 1;
-                        if (W) f[1] = R[1 * RL + ring_idx(Nx, Ny, 0, j)];
-                        if (S) f[2] = R[2 * RL + ring_idx(Nx, Ny, i, 0)];
-                        if (E) f[3] = R[3 * RL + ring_idx(Nx, Ny, Nx + 1, j)];
-                        if (N) f[4] = R[4 * RL + ring_idx(Nx, Ny, i, Ny + 1)];
-                        if (W || S) f[5] = R[5 * RL + ring_idx(Nx, Ny, i - 1, j - 1)];
-                        if (E || S) f[6] = R[6 * RL + ring_idx(Nx, Ny, i + 1, j - 1)];
-                        if (E || N) f[7] = R[7 * RL + ring_idx(Nx, Ny, i + 1, j + 1)];
-                        if (W || N) f[8] = R[8 * RL + ring_idx(Nx, Ny, i - 1, j + 1)];
-                    }
-                } else if (W || E || S || N) {
-                    /* bounce-back values that are not in the stage */
-                    if (S) f[2] = F[4 * pl + cc];
-                    if (N) f[4] = F[2 * pl + cc];
-                    if (W || S) f[5] = F[7 * pl + cc];
-                    if (E || S) f[6] = (E && S) ? corner[0] : F[8 * pl + cc];
-                    if (E || N) f[7] = (E && N) ? corner[1] : F[5 * pl + cc];
-                    if (W || N) f[8] = F[6 * pl + cc];
-                }
-                const int ym = S ? y : y - 1, yp = N ? y : y + 1;
-                g[0] = sg[0 * Gm::RW + col];
-                g[2] = sg[2 * Gm::RW + col];
-                g[4] = sg[4 * Gm::RW + col];
-                if (W) {
-                    g[1] = s.gW[y];
-                    g[5] = s.gW[Ny + ym];
-                    g[8] = s.gW[2 * Ny + yp];
-                } else {
-                    g[1] = sg[1 * Gm::RW + col - 1];
-                    g[5] = sg[5 * Gm::RW + col - 1];
-                    g[8] = sg[8 * Gm::RW + col - 1];
-                }
-                if (E) {
-                    g[3] = c.w[3] * s.tcin[y] * s.pE[y];
-                    g[6] = c.w[6] * s.tcin[ym] * s.pE[Ny + ym];
-                    g[7] = c.w[7] * s.tcin[yp] * s.pE[2 * Ny + yp];
-                } else {
-                    g[3] = sg[3 * Gm::RW + col + 1];
-                    g[6] = sg[6 * Gm::RW + col + 1];
-                    g[7] = sg[7 * Gm::RW + col + 1];
-                }
-                node_f64<TANH, MOM, REF32, RING>(s, c, x, y, cc, E, f, g, ap, am, pc, W || E || S || N);
-#pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    ap[0][k] = ap[1][k]; ap[1][k] = ap[2][k];
-                    am[0][k] = am[1][k]; am[1][k] = am[2][k];
-                }
-                pc[0] = pc[1]; pc[1] = pc[2];
-            }
+            if (active)
+                f64_row<TANH, MOM, REF32, RING>(s, c, corner, stages + (size_t)st * Gm::STAGE_BYTES, x, y, tid, W, E,
+                                                ap, am, pc);
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[st]);
             r++;
@@ -240,6 +260,157 @@ fused_pipe_f64_kernel(StepPtrs<double> s, Consts c, const double *__restrict__ c
         } while (ok && it.t == tile);
         if (failed) break;
     }
+}
+
+/* The FP64 step as a multi-step (dataflow) launch: the schedule of FlowCtl
+ * (pipe_common.cuh) over the consumers above, walls of code 4, no moments;
+ * s0 steps buffer A to B, s1 steps B to A. */
+template <int D, int TANH, bool REF32>
+__global__ void __launch_bounds__(PIPE_THREADS, 3)
+flow_pipe_f64_kernel(StepPtrs<double> s0, StepPtrs<double> s1, Consts c, const double *__restrict__ corner,
+                     PipeSched sch, FlowCtl fl, int *errflag)
+{
+    static_assert(D <= 8, "stage tags hold 8 stages");
+    using Gm = PipeGeom<double, double>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ int warps_done[8];
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem);
+    uint64_t *empty = full + D;
+    StageTag *tag = reinterpret_cast<StageTag *>(smem + 128);
+    unsigned char *stages = smem + Gm::HEADER;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int Nx = c.Nx, Ny = c.Ny;
+    if (tid == 0) {
+        for (int d = 0; d < D; d++) {
+            mbar_init(&full[d], 1);
+            mbar_init(&empty[d], PIPE_CWARPS);
+            warps_done[d] = 0;
+        }
+        mbar_fence_init();
+    }
+    __syncthreads();
+    const long long total = (long long)fl.nsteps * sch.ntiles;
+    if (warp == PIPE_CWARPS) {
+        /* ---------------- producer ---------------- */
+        if (lane != 0) return;
+        long long r = 0;
+        bool bad = false;
+        while (!bad) {
+            const unsigned long long item = atomicAdd(fl.ticket, 1ull);
+            if (item >= (unsigned long long)total) break;
+            const int k = (int)(item / sch.ntiles), t = (int)(item % sch.ntiles);
+            if (k > 0 && !flow_deps(fl.done, t, sch, (unsigned)k, errflag)) {
+                atomicExch(errflag, 4);
+                break;
+            }
+            fence_proxy_async_global();
+            const StepPtrs<double> &sk = (k & 1) ? s1 : s0;
+            const int x0 = (t % sch.nbands) * sch.bx, y0 = (t / sch.nbands) * sch.H;
+            const int y1 = min(y0 + sch.H, Ny);
+            for (int y = y0; y < y1; y++) {
+                const int st = (int)(r % D);
+                if (r >= D && !mbar_wait(&empty[st], (uint32_t)(((r / D) - 1) & 1))) {
+                    atomicExch(errflag, 1);
+                    bad = true;
+                    break;
+                }
+                tag[st] = StageTag{k, t, y, (y == y0 ? TAG_FIRST : 0) | (y == y1 - 1 ? TAG_LAST : 0)};
+                pipe_issue<double, double>(sk.fin, sk.gin, sk.phin, sk.plane, sk.P, Ny, x0, y,
+                                           stages + (size_t)st * Gm::STAGE_BYTES, &full[st]);
+                r++;
+            }
+        }
+        /* a stage with no data tells the consumers to leave */
+        if (!bad) {
+            const int st = (int)(r % D);
+            if (r < D || mbar_wait(&empty[st], (uint32_t)(((r / D) - 1) & 1))) {
+                tag[st] = StageTag{-1, -1, -1, TAG_END};
+                mbar_arrive(&full[st]);
+                r++;
+            } else {
+                atomicExch(errflag, 1);
+            }
+        }
+        /* do not retire while copies into this CTA's shared memory are in flight */
+        for (long long q = (r > D ? r - D : 0); q < r; q++)
+            if (!mbar_wait(&full[q % D], (uint32_t)((q / D) & 1))) atomicExch(errflag, 2);
+        return;
+    }
+    /* ---------------- consumers ---------------- */
+    double ap[3][3], am[3][3], pc[3];
+    for (long long r = 0;; r++) {
+        const int st = (int)(r % D);
+        if (!__all_sync(0xffffffffu, mbar_wait(&full[st], (uint32_t)((r / D) & 1)))) {
+            atomicExch(errflag, 3);
+            break;
+        }
+        const StageTag tg = tag[st];
+        if (tg.flags & TAG_END) break;
+        const StepPtrs<double> &sk = (tg.k & 1) ? s1 : s0;
+        const int x = (tg.t % sch.nbands) * sch.bx + tid;
+        const bool W = (x == 0), E = (x == Nx - 1);
+        if (x < Nx) {
+            if (tg.flags & TAG_FIRST) f64_window_start(sk, Ny, x, tg.y, W, E, ap, am, pc);
+            f64_row<TANH, false, REF32, false>(sk, c, corner, stages + (size_t)st * Gm::STAGE_BYTES, x, tg.y, tid, W,
+                                               E, ap, am, pc);
+        }
+        if (tg.flags & TAG_LAST) {
+            /* this warp's part of the tile is stored; the last of the four
+             * warps publishes the tile's step */
+            __threadfence();
+            __syncwarp();
+            if (lane == 0 && atomicAdd(&warps_done[st], 1) == PIPE_CWARPS - 1) {
+                warps_done[st] = 0;
+                __threadfence();
+                st_release_u32(fl.done + tg.t, (unsigned)tg.k + 1);
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[st]);
+    }
+}
+
+/* nsteps FP64 steps in one dataflow launch (walls of code 4, no moments).
+ * flow_buf: the context's ticket counter and per-tile step counts. */
+template <int T, bool R>
+inline cudaError_t flow_f64_launch_t(bgk_ctx *c, const StepPtrs<double> &s0, const StepPtrs<double> &s1, int nsteps)
+{
+    constexpr int D = 2;
+    using Gm = PipeGeom<double, double>;
+    const size_t smem = Gm::smem_bytes(D);
+    static std::atomic<unsigned long long> done{0};
+    cudaError_t e = pipe_configure(flow_pipe_f64_kernel<D, T, R>, smem, c->dev, done);
+    if (e != cudaSuccess) return e;
+    int grid;
+    const PipeSched sch = pipe_sched(c, c->tune_ctas > 0 ? c->tune_ctas : 3, 4, &grid);
+    const size_t need = sizeof(unsigned long long) + (size_t)sch.ntiles * sizeof(unsigned);
+    if (c->flow_bytes < need) {
+        if (c->flow_buf) cudaFree(c->flow_buf);
+        c->flow_buf = nullptr;
+        c->flow_bytes = 0;
+        if ((e = cudaMalloc(&c->flow_buf, need)) != cudaSuccess) return e;
+        c->flow_bytes = need;
+    }
+    if ((e = cudaMemsetAsync(c->flow_buf, 0, need, c->stream)) != cudaSuccess) return e;
+    FlowCtl fl;
+    fl.ticket = (unsigned long long *)c->flow_buf;
+    fl.done = (unsigned *)((char *)c->flow_buf + sizeof(unsigned long long));
+    fl.nsteps = nsteps;
+    flow_pipe_f64_kernel<D, T, R><<<grid, PIPE_THREADS, smem, c->stream>>>(s0, s1, c->c, c->corner, sch, fl,
+                                                                          c->errflag);
+    return cudaGetLastError();
+}
+
+inline cudaError_t launch_flow_pipe_f64(bgk_ctx *c, const StepPtrs<double> &s0, const StepPtrs<double> &s1,
+                                        int nsteps)
+{
+    const bool portable = c->opt.tanh_mode == BGK_TANH_PORTABLE;
+    const bool ref32 = !c->opt.smooth;
+    if (portable)
+        return ref32 ? flow_f64_launch_t<BGK_TANH_PORTABLE, true>(c, s0, s1, nsteps)
+                     : flow_f64_launch_t<BGK_TANH_PORTABLE, false>(c, s0, s1, nsteps);
+    return ref32 ? flow_f64_launch_t<BGK_TANH_DEVICE, true>(c, s0, s1, nsteps)
+                 : flow_f64_launch_t<BGK_TANH_DEVICE, false>(c, s0, s1, nsteps);
 }
 
 template <int D, int T, bool M, bool R, bool RING = false>

@@ -819,6 +819,35 @@ static int strip_height(const bgk_ctx *c)
     return H;
 }
 
+
+/* Step pointers of a dataflow launch: s0 steps the current buffers into
+ * the other ones, s1 back (no moments written). */
+static void flow_ptrs(const bgk_ctx *c, StepPtrs<double> &s0, StepPtrs<double> &s1)
+{
+    StepPtrs<double> s{};
+    s.gW = c->gW; s.pE = c->pE; s.phiW = c->phiW; s.phiE = c->phiE;
+    s.plane = c->plane; s.P = c->P; s.NX2 = c->NX2;
+    s0 = s;
+    s1 = s;
+    const int a = c->cur, b = c->cur ^ 1;
+    s0.fin = (const double *)c->fbuf[a]; s0.gin = (const double *)c->gbuf[a];
+    s0.fout = (double *)c->fbuf[b]; s0.gout = (double *)c->gbuf[b];
+    s0.phin = (const double *)c->phibuf[a]; s0.phout = (double *)c->phibuf[b];
+    s0.tcin = c->tcol[a]; s0.tcout = c->tcol[b];
+    s1.fin = (const double *)c->fbuf[b]; s1.gin = (const double *)c->gbuf[b];
+    s1.fout = (double *)c->fbuf[a]; s1.gout = (double *)c->gbuf[a];
+    s1.phin = (const double *)c->phibuf[b]; s1.phout = (double *)c->phibuf[a];
+    s1.tcin = c->tcol[b]; s1.tcout = c->tcol[a];
+}
+
+/* nsteps exact-order FP64 steps in one dataflow launch (walls of code 4). */
+cudaError_t launch_flow_f64(bgk_ctx *c, int nsteps)
+{
+    StepPtrs<double> s0, s1;
+    flow_ptrs(c, s0, s1);
+    return launch_flow_pipe_f64(c, s0, s1, nsteps);
+}
+
 cudaError_t launch_fused_f64(bgk_ctx *c, bool moments)
 {
     StepPtrs<double> s{};

@@ -37,6 +37,39 @@ int strip_height(const bgk_ctx *c)
 
 cudaError_t launch_fused_lowp(bgk_ctx *c, bool moments);
 
+
+/* Step pointers of a dataflow launch: s0 steps the current buffers into
+ * the other ones, s1 back (no moments written). */
+static void flow_ptrs(const bgk_ctx *c, StepPtrs<double> &s0, StepPtrs<double> &s1)
+{
+    StepPtrs<double> s{};
+    s.gW = c->gW; s.pE = c->pE; s.phiW = c->phiW; s.phiE = c->phiE;
+    s.plane = c->plane; s.P = c->P; s.NX2 = c->NX2;
+    s0 = s;
+    s1 = s;
+    const int a = c->cur, b = c->cur ^ 1;
+    s0.fin = (const double *)c->fbuf[a]; s0.gin = (const double *)c->gbuf[a];
+    s0.fout = (double *)c->fbuf[b]; s0.gout = (double *)c->gbuf[b];
+    s0.phin = (const double *)c->phibuf[a]; s0.phout = (double *)c->phibuf[b];
+    s0.tcin = c->tcol[a]; s0.tcout = c->tcol[b];
+    s1.fin = (const double *)c->fbuf[b]; s1.gin = (const double *)c->gbuf[b];
+    s1.fout = (double *)c->fbuf[a]; s1.gout = (double *)c->gbuf[a];
+    s1.phin = (const double *)c->phibuf[b]; s1.phout = (double *)c->phibuf[a];
+    s1.tcin = c->tcol[b]; s1.tcout = c->tcol[a];
+}
+
+cudaError_t launch_flow_lowp(bgk_ctx *c, int nsteps);
+
+/* nsteps steps of the FMA-contracted FP64 variant or of a reduced-precision
+ * form in one dataflow launch (walls of code 4, no moments). */
+cudaError_t launch_flow_fast(bgk_ctx *c, int nsteps)
+{
+    if (c->opt.precision != BGK_PREC_F64) return launch_flow_lowp(c, nsteps);
+    StepPtrs<double> s0, s1;
+    flow_ptrs(c, s0, s1);
+    return launch_flow_pipe_f64(c, s0, s1, nsteps);
+}
+
 cudaError_t launch_fused_fast(bgk_ctx *c, bool moments)
 {
     if (c->opt.precision != BGK_PREC_F64) return launch_fused_lowp(c, moments);
@@ -91,6 +124,16 @@ struct ConstsLP {
      * deviations by (1 + 7.45e-9): over 20,000 steps a systematic drift of
      * 1.5e-4 of (T - T0), which moves the melting front. */
     AT wcorr;
+    /* The same rounding scales the first moment of the equilibria:
+     * 3 sum_k w_k c_kx^2 = 1 + 2^-27 for the float weights, so every
+     * collision multiplied the momentum (and the heat flux) by that factor,
+     * a uniform anti-damping force that made the FP32 form's velocity drift
+     * from the FP64 path's in proportion to the step count (6.5e-5 of max
+     * |u| after 10k steps at 4096^2).  mcorr = (3 sum w c^2 - 1)/2 times
+     * rho*u (T*u) is taken from the +x and added to the -x population (and
+     * likewise in y), which leaves the mass and the second moments that the
+     * regularization reads unchanged. */
+    AT mcorr;
     double dts, T0d, rho0d;
     double T0mTcrit_d, inv_T_width_d;
     double w_d[9];
@@ -190,20 +233,8 @@ __device__ __forceinline__ double tanh_pt<double>(double x, int mode)
 /* Phase-field storage.  The update of STEP_7/phase_field.f90:22-48 needs,
  * per cell, the two bases 1 + phi and 1 - phi (of the selector terms
  * (1/2 (1 +- phi))^2 and of the update itself).  A codec gives both for a
- * stored word, phi in double, and the encoding of an updated value.
- *
- * float / double: phi itself.  In FP32 a cell near a pole (phi ~ -1 in the
- * solid, +1 in the liquid) has an ulp of 6e-8, so per-step updates smaller
- * than 3e-8 -- the slow growth of the liquid fraction ahead of the melt
- * front -- round away, and the front lags the FP64 run.
- * PhiQ: 32 bits holding the distance to the nearer pole, signed by the pole:
- * q = -(1 + phi) for phi <= 0 (sign bit set, -0 at phi = -1), q = 1 - phi
- * for phi > 0.  Whichever of 1 +- phi is small is then held to full float
- * precision, and an update of any size changes it. */
-struct PhiQ {
-    float q;
-};
-
+ * stored word, phi in double, and the encoding of an updated value; phi is
+ * stored as itself, in float or in double. */
 template <typename PS> struct PhiCodec;
 template <> struct PhiCodec<float> {
     using A = float;
@@ -225,28 +256,6 @@ template <> struct PhiCodec<double> {
     static __device__ __forceinline__ double update(double s, double kpp, double kmm)
     {
         return s + (0.5 * kpp * (1.0 - s) - 0.5 * kmm * (1.0 + s));
-    }
-};
-template <> struct PhiCodec<PhiQ> {
-    using A = float;
-    static __device__ __forceinline__ float onep(PhiQ s) { return signbit(s.q) ? -s.q : 2.f - s.q; }
-    static __device__ __forceinline__ float onem(PhiQ s) { return signbit(s.q) ? 2.f + s.q : s.q; }
-    static __device__ __forceinline__ double dec(PhiQ s)
-    {
-        return signbit(s.q) ? -1.0 - (double)s.q : 1.0 - (double)s.q;
-    }
-    static __device__ __forceinline__ PhiQ from_d(double phi)
-    {
-        return phi <= 0.0 ? PhiQ{-(float)fabs(1.0 + phi)} : PhiQ{(float)fabs(1.0 - phi)};
-    }
-    /* new phi = phi + d, d = kpp (1 - phi)/2 - kmm (1 + phi)/2, carried on
-     * the small base; a base that rounding takes below zero is a pole */
-    static __device__ __forceinline__ PhiQ update(PhiQ s, float kpp, float kmm)
-    {
-        const float op = onep(s), om = onem(s);
-        const float d = 0.5f * kpp * om - 0.5f * kmm * op;
-        const float opn = op + d, omn = om - d;
-        return opn <= omn ? PhiQ{-fabsf(opn)} : PhiQ{fabsf(omn)};
     }
 };
 
@@ -313,6 +322,11 @@ __device__ __forceinline__ void node_lp(const LpPtrs<S, PT> &s, const ConstsLP<A
 #pragma unroll
     for (int k = 0; k < 9; k++) eq[k] = c.w[k] * (c.rho0 * Q[k] + drho * ((AT)1 + Q[k]));
     eq[0] += c.wcorr * drho;
+    {
+        const AT mx = c.mcorr * rho * u, my = c.mcorr * rho * v;
+        eq[1] -= mx; eq[3] += mx;
+        eq[2] -= my; eq[4] += my;
+    }
     reg_relax_lp(c, f, eq, c.cf, out);
     {
         AT r = drho;                        /* mass closure */
@@ -325,6 +339,11 @@ __device__ __forceinline__ void node_lp(const LpPtrs<S, PT> &s, const ConstsLP<A
 #pragma unroll
     for (int k = 0; k < 9; k++) eq[k] = c.w[k] * (c.T0 * Q[k] + dT * ((AT)1 + Q[k]));
     eq[0] += c.wcorr * dT;
+    {
+        const AT mx = c.mcorr * T * u, my = c.mcorr * T * v;
+        eq[1] -= mx; eq[3] += mx;
+        eq[2] -= my; eq[4] += my;
+    }
     reg_relax_lp(c, g, eq, c.cg, out);
     {
         double r = dTd;                     /* energy closure */
@@ -449,6 +468,115 @@ fused_lowp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, int H, int pf)
     }
 }
 
+/* Pipeline consumers of the reduced-precision step, shared by the
+ * per-step kernel and the multi-step (dataflow) kernel below.
+ *
+ * lp_window_start: the 3x3 phase-field window's first two rows (y0-1, y0)
+ * for column x, from global memory. */
+template <typename S, typename PT, typename AT>
+__device__ __forceinline__ void lp_window_start(const LpPtrs<S, PT> &s, const ConstsLP<AT> &c, int x, int y0,
+                                                bool W, bool E, typename PhiCodec<PT>::A *ap,
+                                                typename PhiCodec<PT>::A *am, PT *pc)
+{
+    using PC = PhiCodec<PT>;
+    using PA = typename PC::A;
+    const PA h = (PA)0.5;
+    const int Ny = c.Ny;
+    for (int slot = 0; slot < 2; slot++) {
+        const int rr = y0 - 1 + slot;
+        const int rc = rr < 0 ? 0 : (rr >= Ny ? Ny - 1 : rr);
+        const PT *row = s.phin + (long long)rc * s.P;
+        const PT pL = W ? PC::from_d(s.phiW[rc]) : row[x - 1];
+        const PT pM = row[x];
+        const PT pR = E ? PC::from_d(s.phiE[rc]) : row[x + 1];
+        const PA a0 = h * PC::onep(pL), a1 = h * PC::onep(pM), a2 = h * PC::onep(pR);
+        const PA b0 = h * PC::onem(pL), b1 = h * PC::onem(pM), b2 = h * PC::onem(pR);
+        ap[slot] = a0 * a0 + a1 * a1 + a2 * a2;
+        am[slot] = b0 * b0 + b1 * b1 + b2 * b2;
+        pc[slot] = pM;
+    }
+}
+
+/* lp_row: node (x, y) from a filled stage: the window's new row y+1, the
+ * pulls (bounce-back and boundary values from global memory), node_lp, and
+ * the window shift. */
+template <typename S, typename PT, typename AT, int TANH, bool MOM>
+__device__ __forceinline__ void lp_row(const LpPtrs<S, PT> &s, const ConstsLP<AT> &c, const unsigned char *stage,
+                                       int x, int y, int tid, bool W, bool E, typename PhiCodec<PT>::A *ap,
+                                       typename PhiCodec<PT>::A *am, PT *pc)
+{
+    using Gm = PipeGeom<S, PT>;
+    using C = Codec<S>;
+    using PC = PhiCodec<PT>;
+    using PA = typename PC::A;
+    const PA h = (PA)0.5;
+    const int Ny = c.Ny;
+    const long long pl = s.plane;
+    const S *__restrict__ F = s.fin;
+    const float isf = s.inv_sf, isg = s.inv_sg;
+    const S *sp = reinterpret_cast<const S *>(stage);
+    const S *sg = sp + 9 * Gm::RW;
+    const PT *sphi = reinterpret_cast<const PT *>(stage + 18 * Gm::POP_BYTES);
+    const bool Sb = (y == 0), N = (y == Ny - 1);
+    const long long cc = (long long)y * s.P + x;
+    const int col = tid + Gm::AL;
+    {
+        const int rc = (y + 1 >= Ny) ? Ny - 1 : y + 1;
+        const PT pL = W ? PC::from_d(s.phiW[rc]) : sphi[Gm::ALP + tid - 1];
+        const PT pM = sphi[Gm::ALP + tid];
+        const PT pR = E ? PC::from_d(s.phiE[rc]) : sphi[Gm::ALP + tid + 1];
+        const PA a0 = h * PC::onep(pL), a1 = h * PC::onep(pM), a2 = h * PC::onep(pR);
+        const PA b0 = h * PC::onem(pL), b1 = h * PC::onem(pM), b2 = h * PC::onem(pR);
+        ap[2] = a0 * a0 + a1 * a1 + a2 * a2;
+        am[2] = b0 * b0 + b1 * b1 + b2 * b2;
+        pc[2] = pM;
+    }
+    AT f[9], g[9];
+    f[0] = (AT)C::lds(sp + 0 * Gm::RW + col, isf);
+    f[1] = (AT)C::lds(W ? sp + 3 * Gm::RW + col : sp + 1 * Gm::RW + col - 1, isf);
+    f[2] = (AT)C::lds(sp + 2 * Gm::RW + col, isf);
+    f[3] = (AT)C::lds(E ? sp + 1 * Gm::RW + col : sp + 3 * Gm::RW + col + 1, isf);
+    f[4] = (AT)C::lds(sp + 4 * Gm::RW + col, isf);
+    f[5] = (AT)C::lds(sp + 5 * Gm::RW + col - 1, isf);
+    f[6] = (AT)C::lds(sp + 6 * Gm::RW + col + 1, isf);
+    f[7] = (AT)C::lds(sp + 7 * Gm::RW + col + 1, isf);
+    f[8] = (AT)C::lds(sp + 8 * Gm::RW + col - 1, isf);
+    if (W || E || Sb || N) {
+        if (Sb) f[2] = (AT)C::ld(F + 4 * pl + cc, isf);
+        if (N) f[4] = (AT)C::ld(F + 2 * pl + cc, isf);
+        if (W || Sb) f[5] = (AT)C::ld(F + 7 * pl + cc, isf);
+        if (E || Sb) f[6] = (E && Sb) ? (AT)(s.corner[0] - c.w_d[6] * c.rho0d) : (AT)C::ld(F + 8 * pl + cc, isf);
+        if (E || N) f[7] = (E && N) ? (AT)(s.corner[1] - c.w_d[7] * c.rho0d) : (AT)C::ld(F + 5 * pl + cc, isf);
+        if (W || N) f[8] = (AT)C::ld(F + 6 * pl + cc, isf);
+    }
+    const int ym = Sb ? y : y - 1, yp = N ? y : y + 1;
+    g[0] = (AT)C::lds(sg + 0 * Gm::RW + col, isg);
+    g[2] = (AT)C::lds(sg + 2 * Gm::RW + col, isg);
+    g[4] = (AT)C::lds(sg + 4 * Gm::RW + col, isg);
+    if (W) {
+        g[1] = (AT)(s.gW[y] - c.w_d[1] * c.T0d);
+        g[5] = (AT)(s.gW[Ny + ym] - c.w_d[5] * c.T0d);
+        g[8] = (AT)(s.gW[2 * Ny + yp] - c.w_d[8] * c.T0d);
+    } else {
+        g[1] = (AT)C::lds(sg + 1 * Gm::RW + col - 1, isg);
+        g[5] = (AT)C::lds(sg + 5 * Gm::RW + col - 1, isg);
+        g[8] = (AT)C::lds(sg + 8 * Gm::RW + col - 1, isg);
+    }
+    if (E) {
+        g[3] = (AT)(c.w_d[3] * s.tcin[y] * s.pE[y] - c.w_d[3] * c.T0d);
+        g[6] = (AT)(c.w_d[6] * s.tcin[ym] * s.pE[Ny + ym] - c.w_d[6] * c.T0d);
+        g[7] = (AT)(c.w_d[7] * s.tcin[yp] * s.pE[2 * Ny + yp] - c.w_d[7] * c.T0d);
+    } else {
+        g[3] = (AT)C::lds(sg + 3 * Gm::RW + col + 1, isg);
+        g[6] = (AT)C::lds(sg + 6 * Gm::RW + col + 1, isg);
+        g[7] = (AT)C::lds(sg + 7 * Gm::RW + col + 1, isg);
+    }
+    node_lp<S, PT, AT, TANH, MOM>(s, c, x, y, cc, E, f, g, (ap[0] + ap[1]) + ap[2], (am[0] + am[1]) + am[2], pc[1]);
+    ap[0] = ap[1]; ap[1] = ap[2];
+    am[0] = am[1]; am[1] = am[2];
+    pc[0] = pc[1]; pc[1] = pc[2];
+}
+
 /* The reduced-precision step on the shared-memory pipeline of
  * fused_pipe.cuh: identical producer, consumers decode deviations from the
  * stage and call node_lp. */
@@ -457,7 +585,6 @@ __global__ void __launch_bounds__(PIPE_THREADS, 4)
 fused_pipe_lp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, PipeSched sch, int *errflag)
 {
     using Gm = PipeGeom<S, PT>;
-    using C = Codec<S>;
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *full = reinterpret_cast<uint64_t *>(smem);
     uint64_t *empty = full + D;
@@ -494,13 +621,7 @@ fused_pipe_lp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, PipeSched sch, int *errfla
         pdl_allow_next();
         return;
     }
-    using PC = PhiCodec<PT>;
-    using PA = typename PC::A;
-    const long long pl = s.plane;
-    const int P = s.P;
-    const S *__restrict__ F = s.fin;
-    const PT *__restrict__ PH = s.phin;
-    const float isf = s.inv_sf, isg = s.inv_sg;
+    using PA = typename PhiCodec<PT>::A;
     PipeIter it;
     long long r = 0;
     bool ok = it.start(sch, Ny);
@@ -510,22 +631,7 @@ fused_pipe_lp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, PipeSched sch, int *errfla
         const bool W = (x == 0), E = (x == Nx - 1);
         PA ap[3], am[3];   /* per row y-1, y, y+1: sums over x-1..x+1 of (1/2 (1 +- phi))^2 */
         PT pc[3];          /* and the stored phi of column x */
-        const PA h = (PA)0.5;
-        if (active) {
-            for (int slot = 0; slot < 2; slot++) {
-                const int rr = it.y - 1 + slot;
-                const int rc = rr < 0 ? 0 : (rr >= Ny ? Ny - 1 : rr);
-                const PT *row = PH + (long long)rc * P;
-                const PT pL = W ? PC::from_d(s.phiW[rc]) : row[x - 1];
-                const PT pM = row[x];
-                const PT pR = E ? PC::from_d(s.phiE[rc]) : row[x + 1];
-                const PA a0 = h * PC::onep(pL), a1 = h * PC::onep(pM), a2 = h * PC::onep(pR);
-                const PA b0 = h * PC::onem(pL), b1 = h * PC::onem(pM), b2 = h * PC::onem(pR);
-                ap[slot] = a0 * a0 + a1 * a1 + a2 * a2;
-                am[slot] = b0 * b0 + b1 * b1 + b2 * b2;
-                pc[slot] = pM;
-            }
-        }
+        if (active) lp_window_start(s, c, x, it.y, W, E, ap, am, pc);
         const int tile = it.t;
         bool failed = false;
         do {
@@ -536,69 +642,9 @@ fused_pipe_lp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, PipeSched sch, int *errfla
                 failed = true;
                 break;
             }
-            const S *sp = reinterpret_cast<const S *>(stages + (size_t)st * Gm::STAGE_BYTES);
-            const S *sg = sp + 9 * Gm::RW;
-            const PT *sphi = reinterpret_cast<const PT *>(stages + (size_t)st * Gm::STAGE_BYTES + 18 * Gm::POP_BYTES);
-            if (active) {
-                const bool Sb = (y == 0), N = (y == Ny - 1);
-                const long long cc = (long long)y * P + x;
-                const int col = tid + Gm::AL;
-                {
-                    const int rc = (y + 1 >= Ny) ? Ny - 1 : y + 1;
-                    const PT pL = W ? PC::from_d(s.phiW[rc]) : sphi[Gm::ALP + tid - 1];
-                    const PT pM = sphi[Gm::ALP + tid];
-                    const PT pR = E ? PC::from_d(s.phiE[rc]) : sphi[Gm::ALP + tid + 1];
-                    const PA a0 = h * PC::onep(pL), a1 = h * PC::onep(pM), a2 = h * PC::onep(pR);
-                    const PA b0 = h * PC::onem(pL), b1 = h * PC::onem(pM), b2 = h * PC::onem(pR);
-                    ap[2] = a0 * a0 + a1 * a1 + a2 * a2;
-                    am[2] = b0 * b0 + b1 * b1 + b2 * b2;
-                    pc[2] = pM;
-                }
-                AT f[9], g[9];
-                f[0] = (AT)C::lds(sp + 0 * Gm::RW + col, isf);
-                f[1] = (AT)C::lds(W ? sp + 3 * Gm::RW + col : sp + 1 * Gm::RW + col - 1, isf);
-                f[2] = (AT)C::lds(sp + 2 * Gm::RW + col, isf);
-                f[3] = (AT)C::lds(E ? sp + 1 * Gm::RW + col : sp + 3 * Gm::RW + col + 1, isf);
-                f[4] = (AT)C::lds(sp + 4 * Gm::RW + col, isf);
-                f[5] = (AT)C::lds(sp + 5 * Gm::RW + col - 1, isf);
-                f[6] = (AT)C::lds(sp + 6 * Gm::RW + col + 1, isf);
-                f[7] = (AT)C::lds(sp + 7 * Gm::RW + col + 1, isf);
-                f[8] = (AT)C::lds(sp + 8 * Gm::RW + col - 1, isf);
-                if (W || E || Sb || N) {
-                    if (Sb) f[2] = (AT)C::ld(F + 4 * pl + cc, isf);
-                    if (N) f[4] = (AT)C::ld(F + 2 * pl + cc, isf);
-                    if (W || Sb) f[5] = (AT)C::ld(F + 7 * pl + cc, isf);
-                    if (E || Sb) f[6] = (E && Sb) ? (AT)(s.corner[0] - c.w_d[6] * c.rho0d) : (AT)C::ld(F + 8 * pl + cc, isf);
-                    if (E || N) f[7] = (E && N) ? (AT)(s.corner[1] - c.w_d[7] * c.rho0d) : (AT)C::ld(F + 5 * pl + cc, isf);
-                    if (W || N) f[8] = (AT)C::ld(F + 6 * pl + cc, isf);
-                }
-                const int ym = Sb ? y : y - 1, yp = N ? y : y + 1;
-                g[0] = (AT)C::lds(sg + 0 * Gm::RW + col, isg);
-                g[2] = (AT)C::lds(sg + 2 * Gm::RW + col, isg);
-                g[4] = (AT)C::lds(sg + 4 * Gm::RW + col, isg);
-                if (W) {
-                    g[1] = (AT)(s.gW[y] - c.w_d[1] * c.T0d);
-                    g[5] = (AT)(s.gW[Ny + ym] - c.w_d[5] * c.T0d);
-                    g[8] = (AT)(s.gW[2 * Ny + yp] - c.w_d[8] * c.T0d);
-                } else {
-                    g[1] = (AT)C::lds(sg + 1 * Gm::RW + col - 1, isg);
-                    g[5] = (AT)C::lds(sg + 5 * Gm::RW + col - 1, isg);
-                    g[8] = (AT)C::lds(sg + 8 * Gm::RW + col - 1, isg);
-                }
-                if (E) {
-                    g[3] = (AT)(c.w_d[3] * s.tcin[y] * s.pE[y] - c.w_d[3] * c.T0d);
-                    g[6] = (AT)(c.w_d[6] * s.tcin[ym] * s.pE[Ny + ym] - c.w_d[6] * c.T0d);
-                    g[7] = (AT)(c.w_d[7] * s.tcin[yp] * s.pE[2 * Ny + yp] - c.w_d[7] * c.T0d);
-                } else {
-                    g[3] = (AT)C::lds(sg + 3 * Gm::RW + col + 1, isg);
-                    g[6] = (AT)C::lds(sg + 6 * Gm::RW + col + 1, isg);
-                    g[7] = (AT)C::lds(sg + 7 * Gm::RW + col + 1, isg);
-                }
-                node_lp<S, PT, AT, TANH, MOM>(s, c, x, y, cc, E, f, g, (ap[0] + ap[1]) + ap[2], (am[0] + am[1]) + am[2], pc[1]);
-                ap[0] = ap[1]; ap[1] = ap[2];
-                am[0] = am[1]; am[1] = am[2];
-                pc[0] = pc[1]; pc[1] = pc[2];
-            }
+            if (active)
+                lp_row<S, PT, AT, TANH, MOM>(s, c, stages + (size_t)st * Gm::STAGE_BYTES, x, y, tid, W, E, ap, am,
+                                             pc);
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[st]);
             r++;
@@ -607,6 +653,115 @@ fused_pipe_lp_kernel(LpPtrs<S, PT> s, ConstsLP<AT> c, PipeSched sch, int *errfla
         if (failed) break;
     }
     pdl_allow_next();
+}
+
+/* Multi-step (dataflow) form of the reduced-precision pipeline: the
+ * schedule, its ordering and its waits are described with FlowCtl in
+ * pipe_common.cuh. */
+template <typename S, typename PT, typename AT, int D, int TANH>
+__global__ void __launch_bounds__(PIPE_THREADS, 4)
+flow_pipe_lp_kernel(LpPtrs<S, PT> s0, LpPtrs<S, PT> s1, ConstsLP<AT> c, PipeSched sch, FlowCtl fl, int *errflag)
+{
+    static_assert(D <= 8, "stage tags hold 8 stages");
+    using Gm = PipeGeom<S, PT>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ int warps_done[8];
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem);
+    uint64_t *empty = full + D;
+    StageTag *tag = reinterpret_cast<StageTag *>(smem + 128);
+    unsigned char *stages = smem + Gm::HEADER;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int Nx = c.Nx, Ny = c.Ny;
+    if (tid == 0) {
+        for (int d = 0; d < D; d++) {
+            mbar_init(&full[d], 1);
+            mbar_init(&empty[d], PIPE_CWARPS);
+            warps_done[d] = 0;
+        }
+        mbar_fence_init();
+    }
+    __syncthreads();
+    const long long total = (long long)fl.nsteps * sch.ntiles;
+    if (warp == PIPE_CWARPS) {
+        /* ---------------- producer ---------------- */
+        if (lane != 0) return;
+        long long r = 0;
+        bool bad = false;
+        while (!bad) {
+            const unsigned long long item = atomicAdd(fl.ticket, 1ull);
+            if (item >= (unsigned long long)total) break;
+            const int k = (int)(item / sch.ntiles), t = (int)(item % sch.ntiles);
+            if (k > 0 && !flow_deps(fl.done, t, sch, (unsigned)k, errflag)) {
+                atomicExch(errflag, 4);
+                break;
+            }
+            fence_proxy_async_global();
+            const LpPtrs<S, PT> &sk = (k & 1) ? s1 : s0;
+            const int x0 = (t % sch.nbands) * sch.bx, y0 = (t / sch.nbands) * sch.H;
+            const int y1 = min(y0 + sch.H, Ny);
+            for (int y = y0; y < y1; y++) {
+                const int st = (int)(r % D);
+                if (r >= D && !mbar_wait(&empty[st], (uint32_t)(((r / D) - 1) & 1))) {
+                    atomicExch(errflag, 1);
+                    bad = true;
+                    break;
+                }
+                tag[st] = StageTag{k, t, y, (y == y0 ? TAG_FIRST : 0) | (y == y1 - 1 ? TAG_LAST : 0)};
+                pipe_issue<S, PT>(sk.fin, sk.gin, sk.phin, sk.plane, sk.P, Ny, x0, y,
+                                  stages + (size_t)st * Gm::STAGE_BYTES, &full[st]);
+                r++;
+            }
+        }
+        /* a stage with no data tells the consumers to leave */
+        if (!bad) {
+            const int st = (int)(r % D);
+            if (r < D || mbar_wait(&empty[st], (uint32_t)(((r / D) - 1) & 1))) {
+                tag[st] = StageTag{-1, -1, -1, TAG_END};
+                mbar_arrive(&full[st]);
+                r++;
+            } else {
+                atomicExch(errflag, 1);
+            }
+        }
+        /* do not retire while copies into this CTA's shared memory are in flight */
+        for (long long q = (r > D ? r - D : 0); q < r; q++)
+            if (!mbar_wait(&full[q % D], (uint32_t)((q / D) & 1))) atomicExch(errflag, 2);
+        return;
+    }
+    /* ---------------- consumers ---------------- */
+    using PA = typename PhiCodec<PT>::A;
+    PA ap[3], am[3];
+    PT pc[3];
+    for (long long r = 0;; r++) {
+        const int st = (int)(r % D);
+        if (!__all_sync(0xffffffffu, mbar_wait(&full[st], (uint32_t)((r / D) & 1)))) {
+            atomicExch(errflag, 3);
+            break;
+        }
+        const StageTag tg = tag[st];
+        if (tg.flags & TAG_END) break;
+        const LpPtrs<S, PT> &sk = (tg.k & 1) ? s1 : s0;
+        const int x = (tg.t % sch.nbands) * sch.bx + tid;
+        const bool W = (x == 0), E = (x == Nx - 1);
+        if (x < Nx) {
+            if (tg.flags & TAG_FIRST) lp_window_start(sk, c, x, tg.y, W, E, ap, am, pc);
+            lp_row<S, PT, AT, TANH, false>(sk, c, stages + (size_t)st * Gm::STAGE_BYTES, x, tg.y, tid, W, E, ap, am,
+                                           pc);
+        }
+        if (tg.flags & TAG_LAST) {
+            /* this warp's part of the tile is stored; the last of the four
+             * warps publishes the tile's step */
+            __threadfence();
+            __syncwarp();
+            if (lane == 0 && atomicAdd(&warps_done[st], 1) == PIPE_CWARPS - 1) {
+                warps_done[st] = 0;
+                __threadfence();
+                st_release_u32(fl.done + tg.t, (unsigned)tg.k + 1);
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[st]);
+    }
 }
 
 template <typename S, typename PT, typename AT, int D, int T, bool M>
@@ -743,6 +898,9 @@ ConstsLP<AT> make_lp(const bgk_ctx *b)
         double ws = 0.0;   /* exact: nine floats of similar size sum without rounding in double */
         for (int k = 0; k < 9; k++) ws += (double)l.w[k];
         l.wcorr = (AT)(1.0 - ws);
+        /* 2 w1 + 4 w5 and three times it are exact in double */
+        const double m = 3.0 * (2.0 * (double)l.w[1] + 4.0 * (double)l.w[5]) - 1.0;
+        l.mcorr = (AT)(0.5 * m);
     }
     l.dts = c.dts;
     l.T0mTcrit_d = c.T0 - c.T_crit - c.T_act;
@@ -789,18 +947,75 @@ cudaError_t launch_lowp_t(bgk_ctx *c, bool moments)
     return cudaGetLastError();
 }
 
+/* nsteps steps of a reduced-precision form in one dataflow launch (no
+ * moments written); the state advances from buffer cur to cur ^ (nsteps & 1). */
+template <typename S, typename PT, typename AT>
+cudaError_t launch_flow_t(bgk_ctx *c, int nsteps)
+{
+    constexpr int D = 4;
+    LpPtrs<S, PT> s0{};
+    const int a = c->cur, b = c->cur ^ 1;
+    s0.gW = c->gW; s0.pE = c->pE; s0.phiW = c->phiW; s0.phiE = c->phiE; s0.corner = c->corner;
+    s0.plane = c->plane; s0.P = c->P; s0.NX2 = c->NX2;
+    s0.sf = c->scale.sf; s0.sg = c->scale.sg; s0.inv_sf = c->scale.inv_sf; s0.inv_sg = c->scale.inv_sg;
+    LpPtrs<S, PT> s1 = s0;
+    s0.fin = (const S *)c->fbuf[a]; s0.gin = (const S *)c->gbuf[a]; s0.fout = (S *)c->fbuf[b]; s0.gout = (S *)c->gbuf[b];
+    s0.phin = (const PT *)c->phibuf[a]; s0.phout = (PT *)c->phibuf[b]; s0.tcin = c->tcol[a]; s0.tcout = c->tcol[b];
+    s1.fin = (const S *)c->fbuf[b]; s1.gin = (const S *)c->gbuf[b]; s1.fout = (S *)c->fbuf[a]; s1.gout = (S *)c->gbuf[a];
+    s1.phin = (const PT *)c->phibuf[b]; s1.phout = (PT *)c->phibuf[a]; s1.tcin = c->tcol[b]; s1.tcout = c->tcol[a];
+    const ConstsLP<AT> lp = make_lp<AT>(c);
+    int grid;
+    const PipeSched sch = pipe_sched(c, c->tune_ctas > 0 ? c->tune_ctas : 4, 8, &grid);
+    const size_t need = sizeof(unsigned long long) + (size_t)sch.ntiles * sizeof(unsigned);
+    if (c->flow_bytes < need) {
+        if (c->flow_buf) cudaFree(c->flow_buf);
+        c->flow_buf = nullptr;
+        c->flow_bytes = 0;
+        cudaError_t e = cudaMalloc(&c->flow_buf, need);
+        if (e != cudaSuccess) return e;
+        c->flow_bytes = need;
+    }
+    cudaError_t e = cudaMemsetAsync(c->flow_buf, 0, need, c->stream);
+    if (e != cudaSuccess) return e;
+    FlowCtl fl;
+    fl.ticket = (unsigned long long *)c->flow_buf;
+    fl.done = (unsigned *)((char *)c->flow_buf + sizeof(unsigned long long));
+    fl.nsteps = nsteps;
+    using Gm = PipeGeom<S, PT>;
+    const size_t smem = Gm::smem_bytes(D);
+    if (c->opt.tanh_mode == BGK_TANH_PORTABLE) {
+        static std::atomic<unsigned long long> done{0};
+        if ((e = pipe_configure(flow_pipe_lp_kernel<S, PT, AT, D, BGK_TANH_PORTABLE>, smem, c->dev, done))) return e;
+        flow_pipe_lp_kernel<S, PT, AT, D, BGK_TANH_PORTABLE><<<grid, PIPE_THREADS, smem, c->stream>>>(s0, s1, lp, sch,
+                                                                                                     fl, c->errflag);
+    } else {
+        static std::atomic<unsigned long long> done{0};
+        if ((e = pipe_configure(flow_pipe_lp_kernel<S, PT, AT, D, BGK_TANH_DEVICE>, smem, c->dev, done))) return e;
+        flow_pipe_lp_kernel<S, PT, AT, D, BGK_TANH_DEVICE><<<grid, PIPE_THREADS, smem, c->stream>>>(s0, s1, lp, sch,
+                                                                                                   fl, c->errflag);
+    }
+    return cudaGetLastError();
+}
+
 } // namespace
 
+cudaError_t launch_flow_lowp(bgk_ctx *c, int nsteps)
+{
+    const bool p64 = c->phisz == 8;
+    if (c->opt.precision == BGK_PREC_F32X) return launch_flow_t<float, double, double>(c, nsteps);
+    if (c->opt.precision == BGK_PREC_F32)
+        return p64 ? launch_flow_t<float, double, float>(c, nsteps) : launch_flow_t<float, float, float>(c, nsteps);
+    return p64 ? launch_flow_t<__half, double, float>(c, nsteps) : launch_flow_t<__half, float, float>(c, nsteps);
+}
+
 cudaError_t launch_fused_lowp(bgk_ctx *c, bool moments)
+
 {
     const bool p64 = c->phisz == 8;
     if (c->opt.precision == BGK_PREC_F32X) return launch_lowp_t<float, double, double>(c, moments);
-    if (c->opt.precision == BGK_PREC_F32) {
-        if (p64) return launch_lowp_t<float, double, float>(c, moments);
-        return c->phi_pole ? launch_lowp_t<float, PhiQ, float>(c, moments) : launch_lowp_t<float, float, float>(c, moments);
-    }
-    if (p64) return launch_lowp_t<__half, double, float>(c, moments);
-    return c->phi_pole ? launch_lowp_t<__half, PhiQ, float>(c, moments) : launch_lowp_t<__half, float, float>(c, moments);
+    if (c->opt.precision == BGK_PREC_F32)
+        return p64 ? launch_lowp_t<float, double, float>(c, moments) : launch_lowp_t<float, float, float>(c, moments);
+    return p64 ? launch_lowp_t<__half, double, float>(c, moments) : launch_lowp_t<__half, float, float>(c, moments);
 }
 
 /* FP16 scales: powers of two that put the largest deviations expected in
@@ -839,12 +1054,9 @@ cudaError_t launch_init_lowp(bgk_ctx *c)
     init_lowp_kernel<S, PT><<<grd, blk, 0, c->stream>>>(c->c, (S *)fb, (S *)gb, (PT *)c->phibuf[0],     \
                                                         (PT *)c->phibuf[1], c->plane, c->P, sf_, sg_)
     if (c->opt.precision != BGK_PREC_F16) {
-        if (p64) BGK_INIT(float, double, 1.f, 1.f);
-        else if (c->phi_pole) BGK_INIT(float, PhiQ, 1.f, 1.f);
-        else BGK_INIT(float, float, 1.f, 1.f);
+        if (p64) BGK_INIT(float, double, 1.f, 1.f); else BGK_INIT(float, float, 1.f, 1.f);
     } else {
         if (p64) BGK_INIT(__half, double, c->scale.sf, c->scale.sg);
-        else if (c->phi_pole) BGK_INIT(__half, PhiQ, c->scale.sf, c->scale.sg);
         else BGK_INIT(__half, float, c->scale.sf, c->scale.sg);
     }
 #undef BGK_INIT
@@ -872,8 +1084,6 @@ static int lp_to_compact(bgk_ctx *c, int field, const double *ref)
         for (int b = 0; b < 2; b++) {
             if (c->phisz == 8)
                 phi_ref_to_plane<double><<<grd, blk, 0, c->stream>>>(c->c, ref, (double *)c->phibuf[b], c->P);
-            else if (c->phi_pole)
-                phi_ref_to_plane<PhiQ><<<grd, blk, 0, c->stream>>>(c->c, ref, (PhiQ *)c->phibuf[b], c->P);
             else
                 phi_ref_to_plane<float><<<grd, blk, 0, c->stream>>>(c->c, ref, (float *)c->phibuf[b], c->P);
         }
@@ -903,8 +1113,6 @@ static int lp_to_ref(bgk_ctx *c, int field, double *ref, int prev)
     } else if (field == BGK_FIELD_PHI_PREC) {
         if (c->phisz == 8)
             phi_plane_to_ref<double><<<grd, blk, 0, c->stream>>>(c->c, (const double *)c->phibuf[b], c->P, ref, c->mphi);
-        else if (c->phi_pole)
-            phi_plane_to_ref<PhiQ><<<grd, blk, 0, c->stream>>>(c->c, (const PhiQ *)c->phibuf[b], c->P, ref, c->mphi);
         else
             phi_plane_to_ref<float><<<grd, blk, 0, c->stream>>>(c->c, (const float *)c->phibuf[b], c->P, ref, c->mphi);
     } else {

@@ -166,4 +166,72 @@ inline cudaError_t pdl_launch(void (*kernel)(KArgs...), int grid, int block, siz
     return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
+/* ------------------------------------------------------------------------
+ * Multi-step (dataflow) pipeline kernels (the FP64 step in fused_pipe.cuh,
+ * the reduced-precision forms in kernels_fast.cu).
+ *
+ * One launch advances nsteps steps, so the grid does not drain and refill
+ * at every step boundary.  Work items are (step k, tile t) in step-major
+ * order, taken from a ticket counter by the producer of whichever CTA is
+ * free.  An item may start once the 3x3 tile neighbourhood of t has
+ * completed step k-1 (done[t'] >= k).  That covers every value the item
+ * reads -- pull rows y +- 1, the phase-field stencil, the 16-byte pads into
+ * the neighbouring bands, the east T column at rows y +- 1 -- and, because
+ * the two buffers alternate, every value it overwrites: its own rows of the
+ * buffer that step k-1 pulled from, which only items of that neighbourhood
+ * read.  Every dependency holds a smaller ticket, claimed by a running CTA,
+ * so the smallest unfinished ticket can always proceed and the schedule
+ * needs no co-residency.
+ *
+ * Ordering: the consumers' stores of a tile are fenced (membar.gl) before
+ * the last of its four warps releases done[t]; a producer acquires the
+ * flags, then orders the bulk copies (async proxy) after that with
+ * fence.proxy.async, and hands the stage to its consumers through the
+ * stage's mbarrier.  Every wait is bounded; on expiry the error flag is set
+ * and every CTA leaves.
+ * ---------------------------------------------------------------------- */
+struct FlowCtl {
+    unsigned long long *ticket; /* next work item (zero at launch)         */
+    unsigned *done;     /* [ntiles]: steps completed by each tile (zero)   */
+    int nsteps;
+};
+struct StageTag {
+    int k, t, y, flags;
+};
+constexpr int TAG_FIRST = 1, TAG_LAST = 2, TAG_END = 4;
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned *p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+
+/* Wait (bounded) until every tile of the 3x3 neighbourhood of t has done
+ * `need` steps; false on expiry or once another CTA raised the error flag. */
+__device__ bool flow_deps(const unsigned *done, int t, const PipeSched &sch, unsigned need, const int *errflag)
+{
+    const int b = t % sch.nbands, st = t / sch.nbands;
+    for (int ds = -1; ds <= 1; ds++) {
+        const int ss = st + ds;
+        if (ss < 0 || ss >= sch.nstrips) continue;
+        for (int db = -1; db <= 1; db++) {
+            const int bb = b + db;
+            if (bb < 0 || bb >= sch.nbands) continue;
+            const unsigned *p = done + (long long)ss * sch.nbands + bb;
+            for (long long i = 0; ld_acquire_u32(p) < need; i++) {
+                if (i > PIPE_WAIT_LIMIT) return false;
+                if ((i & 255) == 255 && *(volatile const int *)errflag) return false;
+                if (i > 32) __nanosleep(64);
+            }
+        }
+    }
+    return true;
+}
+
 #endif

@@ -264,3 +264,34 @@ def test_smooth_form_bit_exact(oracle_mod, lib, Nx, Ny):
     # and it differs from the reference roundings
     r = oracle_mod.Oracle(p, tanh="portable"); r.initialization(); r.step(20)
     assert not np.array_equal(r.field("T"), o.field("T"))
+
+
+@pytest.mark.parametrize("Nx,Ny", [(16, 12), (131, 37), (1, 5), (6, 1), (300, 257)])
+def test_dataflow_fp64_bit_exact(oracle_mod, lib, monkeypatch, Nx, Ny):
+    """The multi-step (dataflow) launch of the FP64 step (BGK_FLOW=1): tiles
+    of later steps start as soon as their 3x3 neighbourhood has finished the
+    previous step; the node arithmetic is the per-step kernel's, so the
+    result equals the oracle bit for bit."""
+    monkeypatch.setenv("BGK_FLOW", "1")
+    o, s = make_pair(oracle_mod, lib, Nx, Ny)
+    for n in (23, 2, 9):
+        o.step(n)
+        s.step(n)
+        s.sync()
+        assert_fused_equal(o, s, f"after {o.it} steps")
+
+
+def test_dataflow_fp64_fma_matches_per_step_launches(lib, monkeypatch):
+    """The FMA variant in the dataflow launch equals its per-step launches."""
+    from bgk_pcm_b200 import Solver
+    p = small_params(200, 150)
+    out = []
+    for flow in ("0", "1"):
+        monkeypatch.setenv("BGK_FLOW", flow)
+        with Solver(p, fma=True) as s:
+            s.initialization()
+            s.step(41)
+            s.sync()
+            out.append({n: s.field(n) for n in MACRO + ["f5", "g2"]})
+    for n in out[0]:
+        np.testing.assert_array_equal(out[1][n], out[0][n], err_msg=n)

@@ -139,3 +139,28 @@ def test_register_pull_and_pipeline_agree(lib, monkeypatch, precision):
     b = run(precision, p, 25)
     for n in a:
         np.testing.assert_array_equal(a[n], b[n], err_msg=n)
+
+
+@pytest.mark.parametrize("precision,phi64", [("f32", "0"), ("f32", "1"), ("f16", "0"), ("f32x", "0")])
+@pytest.mark.parametrize("Nx,Ny", [(16, 12), (131, 37), (6, 1), (1, 5), (300, 257)])
+def test_dataflow_steps_bit_identical(lib, monkeypatch, precision, phi64, Nx, Ny):
+    """The multi-step (dataflow) launch computes every node with the same
+    device functions, in the same order of operations, as one launch per
+    step, so the two give the same bits; only the schedule differs (tiles of
+    later steps start as soon as their neighbourhood is done)."""
+    from bgk_pcm_b200 import Solver
+    p = small_params(Nx, Ny)
+    monkeypatch.setenv("BGK_LP_PHI64", phi64)
+    outs = []
+    for flow in ("0", "1"):
+        monkeypatch.setenv("BGK_FLOW", flow)
+        with Solver(p, precision=precision) as s:
+            s.initialization()
+            s.step(23)
+            s.step(2)
+            s.step(9)
+            s.sync()
+            assert s.it == 34
+            outs.append({n: s.field(n) for n in ("rho", "T", "u", "v", "phi", "phi_prec", "f3", "g7")})
+    for n in outs[0]:
+        np.testing.assert_array_equal(outs[1][n], outs[0][n], err_msg=n)
