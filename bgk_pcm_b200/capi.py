@@ -25,7 +25,7 @@ ERRORS = {
 }
 
 PREC_F64, PREC_F32, PREC_F16, PREC_F32X = 0, 1, 2, 3
-TANH_DEVICE, TANH_PORTABLE = 0, 1
+TANH_PORTABLE, TANH_DEVICE = 0, 1
 
 FIELD_F0, FIELD_G0 = 0, 9
 FIELD_RHO, FIELD_T, FIELD_U, FIELD_V = 18, 19, 20, 21

@@ -381,10 +381,12 @@ int bgk_create(const bgk_params *pp, const bgk_options *opt, bgk_ctx **out)
     *out = nullptr;
     int rc = check_params(*pp);
     if (rc) return rc;
-    bgk_options o{BGK_PREC_F64, BGK_TANH_DEVICE, 0, -1, 0};
+    bgk_options o{BGK_PREC_F64, BGK_TANH_PORTABLE, 0, -1, 0};
     if (opt) o = *opt;
     if (o.precision < BGK_PREC_F64 || o.precision > BGK_PREC_F32X) return fail(BGK_ERR_ARG, "bad precision %d", o.precision);
     if (o.tanh_mode != BGK_TANH_DEVICE && o.tanh_mode != BGK_TANH_PORTABLE) return fail(BGK_ERR_ARG, "bad tanh_mode");
+    /* the FP32 and FP16 forms are bit-exact with nothing: CUDA's tanhf */
+    if (o.precision == BGK_PREC_F32 || o.precision == BGK_PREC_F16) o.tanh_mode = BGK_TANH_DEVICE;
     if (o.precision != BGK_PREC_F64 && !all_bc4(*pp))
         return fail(BGK_ERR_UNSUPPORTED, "reduced-precision forms implement the no-slip code 4 on every wall only");
 

@@ -30,7 +30,7 @@ def _dptr(a: np.ndarray):
 class Solver:
     """One simulation on one B200 (STEP_7/setup.f90 allocates, this creates)."""
 
-    def __init__(self, params, precision: str = "f64", tanh: str = "device", fma: bool = False,
+    def __init__(self, params, precision: str = "f64", tanh: str = "portable", fma: bool = False,
                  device: int = -1, smooth: bool = False):
         lib = capi.load()
         if isinstance(params, dict):

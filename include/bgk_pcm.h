@@ -58,13 +58,18 @@ typedef struct bgk_params {
 #define BGK_PREC_F16   2  /* FP16 deviations with a per-field scale, FP32 math          */
 #define BGK_PREC_F32X  3  /* FP32 deviations, FP64 math, phi in FP64                   */
 
-/* tanh used by the phase-field selector (STEP_7/phase_field.f90:20-21). */
-#define BGK_TANH_DEVICE   0  /* CUDA's tanh (production)                              */
-#define BGK_TANH_PORTABLE 1  /* bgk_portable_tanh.h: bit-identical CPU/GPU check mode */
+/* tanh used by the phase-field selector (STEP_7/phase_field.f90:20-21) in
+ * the FP64 forms (BGK_PREC_F64, BGK_PREC_F32X).  The default, portable tanh
+ * (bgk_portable_tanh.h, a few ulp from libm) is evaluated the same way by the
+ * CPU oracle, so the FP64 step equals it bit for bit; it costs 1.4-2.5 % of
+ * the step's throughput on B200 against CUDA's tanh.  The FP32 and FP16 forms
+ * always use CUDA's tanhf. */
+#define BGK_TANH_PORTABLE 0  /* bit-identical to the CPU oracle (default)          */
+#define BGK_TANH_DEVICE   1  /* CUDA's tanh                                         */
 
 typedef struct bgk_options {
     int precision;   /* BGK_PREC_*                                              */
-    int tanh_mode;   /* BGK_TANH_*                                              */
+    int tanh_mode;   /* BGK_TANH_* (FP64 forms)                                 */
     int fma;         /* FP64 only: 0 = the reference's exact operation order    */
                      /* (no fused multiply-add); 1 = FMA-contracted variant      */
     int device;      /* CUDA device ordinal, or -1 for the current device        */
@@ -105,10 +110,15 @@ int bgk_read_input(const char *path, bgk_params *out);
 
 /* Allocate device state and derive the constants (weights, omega_f, omega_g,
  * kvisc, alpha).  Replaces STEP_7/setup.f90:34-115.  opt may be NULL
- * (FP64, device tanh, exact order, current device).  The fused step supports
- * the no-slip code 4 on all four walls, the only code any shipped input uses
- * (UTIL/input.dat.0-3); the staged entry points also run BC_f codes
- * 0/1/2/3/5/6 (FP64 only). */
+ * (FP64, portable tanh, exact order, current device: the same as a
+ * zero-initialized bgk_options).  Walls: the FP64 step (fused and staged)
+ * runs every BC_f code of STEP_7/BC_f.f90 (0 periodic, 1 fixed velocity, 2
+ * parabolic inflow, 3 fixed pressure, 4 no-slip, 5 symmetric, 6 open); with
+ * a wall other than code 4 the fused step keeps the f halo cells in a ring
+ * that a one-block kernel updates before each step as BC_f does.  The
+ * reduced-precision forms, bgk_advance, the packed-row exchange and the
+ * adjoint implement the no-slip code 4, the only code any shipped input
+ * uses (UTIL/input.dat.0-3). */
 int bgk_create(const bgk_params *p, const bgk_options *opt, bgk_ctx **out);
 int bgk_destroy(bgk_ctx *ctx);
 
