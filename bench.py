@@ -415,8 +415,8 @@ def main():
     ap.add_argument("--precision", default="f64", choices=["f64", "f32", "f16", "f32x"])
     ap.add_argument("--tanh", default="portable", choices=["portable", "device"],
                     help="phase-field tanh: the portable one (bit-identical to the oracle) or CUDA's")
-    ap.add_argument("--forms", default="f64device,f64fma,f32,f16,f32x",
-                    help="extra forms timed beside the headline (comma list)")
+    ap.add_argument("--forms", default="f64device,f64fma,f32,f32x",
+                    help="extra forms timed beside the headline (comma list; f16 also exists)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward cost leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")

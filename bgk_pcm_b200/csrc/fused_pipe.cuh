@@ -46,6 +46,9 @@ struct PipeGeom {
     static constexpr int TX_BYTES = 18 * POP_BYTES + PHI_BYTES;
     static constexpr int HEADER = 256;                    /* mbarriers (2 x 16 max) */
     static size_t smem_bytes(int D) { return (size_t)HEADER + (size_t)D * STAGE_BYTES; }
+    /* dataflow stages also carry a tile's first two window rows of phi */
+    static constexpr int STAGE_BYTES_W = (18 * POP_BYTES + 3 * PHI_BYTES + 127) / 128 * 128;
+    static size_t smem_bytes_w(int D) { return (size_t)HEADER + (size_t)D * STAGE_BYTES_W; }
 };
 
 __constant__ int pipe_cy[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
@@ -185,6 +188,52 @@ __device__ __forceinline__ void f64_row(const StepPtrs<double> &s, const Consts 
     pc[0] = pc[1]; pc[1] = pc[2];
 }
 
+/* Dataflow producer: as pipe_issue, and on a tile's first row y also the
+ * phi rows y-1 (clamped) and y, the window the consumers start the tile
+ * with, into the stage's two extra row slots. */
+template <typename S, typename PT>
+__device__ __forceinline__ void pipe_issue_w(const S *F, const S *G, const PT *PH, long long pl, int P, int Ny,
+                                             int x0, int y, bool first, unsigned char *stage, uint64_t *full)
+{
+    using Gm = PipeGeom<S, PT>;
+    mbar_arrive_expect_tx(full, Gm::TX_BYTES + (first ? 2 * Gm::PHI_BYTES : 0));
+#pragma unroll 1
+    for (int k = 0; k < 9; k++) {
+        int r = y - pipe_cy[k];
+        r = r < 0 ? 0 : (r >= Ny ? Ny - 1 : r);
+        const long long off = (long long)r * P + x0 - Gm::AL;
+        bulk_g2s(stage + k * Gm::POP_BYTES, F + k * pl + off, Gm::POP_BYTES, full);
+        bulk_g2s(stage + (9 + k) * Gm::POP_BYTES, G + k * pl + off, Gm::POP_BYTES, full);
+    }
+    const int rp = (y + 1 >= Ny) ? Ny - 1 : y + 1;
+    unsigned char *sphi = stage + 18 * Gm::POP_BYTES;
+    bulk_g2s(sphi, PH + (long long)rp * P + x0 - Gm::ALP, Gm::PHI_BYTES, full);
+    if (first) {
+        const int rm = y > 0 ? y - 1 : 0;
+        bulk_g2s(sphi + Gm::PHI_BYTES, PH + (long long)rm * P + x0 - Gm::ALP, Gm::PHI_BYTES, full);
+        bulk_g2s(sphi + 2 * Gm::PHI_BYTES, PH + (long long)y * P + x0 - Gm::ALP, Gm::PHI_BYTES, full);
+    }
+}
+
+/* The FP64 window's first two rows from a dataflow stage (slots 1 and 2). */
+__device__ __forceinline__ void f64_window_stage(const StepPtrs<double> &s, int Ny, int y0, int tid, bool W, bool E,
+                                                 const unsigned char *stage, double (&ap)[3][3], double (&am)[3][3],
+                                                 double *pc)
+{
+    using Gm = PipeGeom<double, double>;
+    for (int slot = 0; slot < 2; slot++) {
+        const int rr = y0 - 1 + slot;
+        const int rc = rr < 0 ? 0 : (rr >= Ny ? Ny - 1 : rr);
+        const double *row = reinterpret_cast<const double *>(stage + 18 * Gm::POP_BYTES + (1 + slot) * Gm::PHI_BYTES);
+        const double pL = W ? s.phiW[rc] : row[Gm::ALP + tid - 1];
+        const double pM = row[Gm::ALP + tid];
+        const double pR = E ? s.phiE[rc] : row[Gm::ALP + tid + 1];
+        ap[slot][0] = aplus(pL); ap[slot][1] = aplus(pM); ap[slot][2] = aplus(pR);
+        am[slot][0] = aminus(pL); am[slot][1] = aminus(pM); am[slot][2] = aminus(pR);
+        pc[slot] = pM;
+    }
+}
+
 template <int D, int TANH, bool MOM, bool REF32, bool RING = false>
 __global__ void __launch_bounds__(PIPE_THREADS, 3)
 fused_pipe_f64_kernel(StepPtrs<double> s, Consts c, const double *__restrict__ corner, PipeSched sch, int *errflag)
@@ -295,9 +344,15 @@ flow_pipe_f64_kernel(StepPtrs<double> s0, StepPtrs<double> s1, Consts c, const d
         if (lane != 0) return;
         long long r = 0;
         bool bad = false;
+        /* the next ticket is claimed one tile ahead, so its round trip
+         * overlaps the current tile's copies; a claimed ticket is always
+         * larger than the one in progress, so the schedule stays free of
+         * deadlock */
+        unsigned long long next = atomicAdd(fl.ticket, 1ull);
         while (!bad) {
-            const unsigned long long item = atomicAdd(fl.ticket, 1ull);
+            const unsigned long long item = next;
             if (item >= (unsigned long long)total) break;
+            next = atomicAdd(fl.ticket, 1ull);
             const int k = (int)(item / sch.ntiles), t = (int)(item % sch.ntiles);
             if (k > 0 && !flow_deps(fl.done, t, sch, (unsigned)k, errflag)) {
                 atomicExch(errflag, 4);
@@ -315,8 +370,8 @@ flow_pipe_f64_kernel(StepPtrs<double> s0, StepPtrs<double> s1, Consts c, const d
                     break;
                 }
                 tag[st] = StageTag{k, t, y, (y == y0 ? TAG_FIRST : 0) | (y == y1 - 1 ? TAG_LAST : 0)};
-                pipe_issue<double, double>(sk.fin, sk.gin, sk.phin, sk.plane, sk.P, Ny, x0, y,
-                                           stages + (size_t)st * Gm::STAGE_BYTES, &full[st]);
+                pipe_issue_w<double, double>(sk.fin, sk.gin, sk.phin, sk.plane, sk.P, Ny, x0, y, y == y0,
+                                             stages + (size_t)st * Gm::STAGE_BYTES_W, &full[st]);
                 r++;
             }
         }
@@ -350,19 +405,23 @@ flow_pipe_f64_kernel(StepPtrs<double> s0, StepPtrs<double> s1, Consts c, const d
         const int x = (tg.t % sch.nbands) * sch.bx + tid;
         const bool W = (x == 0), E = (x == Nx - 1);
         if (x < Nx) {
-            if (tg.flags & TAG_FIRST) f64_window_start(sk, Ny, x, tg.y, W, E, ap, am, pc);
-            f64_row<TANH, false, REF32, false>(sk, c, corner, stages + (size_t)st * Gm::STAGE_BYTES, x, tg.y, tid, W,
-                                               E, ap, am, pc);
+            const unsigned char *stg = stages + (size_t)st * Gm::STAGE_BYTES_W;
+            if (tg.flags & TAG_FIRST) f64_window_stage(sk, Ny, tg.y, tid, W, E, stg, ap, am, pc);
+            f64_row<TANH, false, REF32, false>(sk, c, corner, stg, x, tg.y, tid, W, E, ap, am, pc);
         }
         if (tg.flags & TAG_LAST) {
-            /* this warp's part of the tile is stored; the last of the four
-             * warps publishes the tile's step */
-            __threadfence();
+            /* this warp's part of the tile is stored: the warp barrier orders
+             * the lanes' stores before lane 0's fence, whose cumulativity
+             * makes them visible device-wide (the pattern of a grid-wide
+             * barrier); the last of the four warps publishes the tile's step */
             __syncwarp();
-            if (lane == 0 && atomicAdd(&warps_done[st], 1) == PIPE_CWARPS - 1) {
-                warps_done[st] = 0;
+            if (lane == 0) {
                 __threadfence();
-                st_release_u32(fl.done + tg.t, (unsigned)tg.k + 1);
+                if (atomicAdd(&warps_done[st], 1) == PIPE_CWARPS - 1) {
+                    warps_done[st] = 0;
+                    __threadfence();
+                    st_release_u32(fl.done + tg.t, (unsigned)tg.k + 1);
+                }
             }
         }
         __syncwarp();
@@ -377,7 +436,7 @@ inline cudaError_t flow_f64_launch_t(bgk_ctx *c, const StepPtrs<double> &s0, con
 {
     constexpr int D = 2;
     using Gm = PipeGeom<double, double>;
-    const size_t smem = Gm::smem_bytes(D);
+    const size_t smem = Gm::smem_bytes_w(D);
     static std::atomic<unsigned long long> done{0};
     cudaError_t e = pipe_configure(flow_pipe_f64_kernel<D, T, R>, smem, c->dev, done);
     if (e != cudaSuccess) return e;

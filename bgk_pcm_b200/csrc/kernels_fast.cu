@@ -497,6 +497,32 @@ __device__ __forceinline__ void lp_window_start(const LpPtrs<S, PT> &s, const Co
     }
 }
 
+/* lp_window_stage: the same two rows from a dataflow stage (slots 1, 2). */
+template <typename S, typename PT, typename AT>
+__device__ __forceinline__ void lp_window_stage(const LpPtrs<S, PT> &s, const ConstsLP<AT> &c, int y0, int tid, bool W,
+                                                bool E, const unsigned char *stage, typename PhiCodec<PT>::A *ap,
+                                                typename PhiCodec<PT>::A *am, PT *pc)
+{
+    using Gm = PipeGeom<S, PT>;
+    using PC = PhiCodec<PT>;
+    using PA = typename PC::A;
+    const PA h = (PA)0.5;
+    const int Ny = c.Ny;
+    for (int slot = 0; slot < 2; slot++) {
+        const int rr = y0 - 1 + slot;
+        const int rc = rr < 0 ? 0 : (rr >= Ny ? Ny - 1 : rr);
+        const PT *row = reinterpret_cast<const PT *>(stage + 18 * Gm::POP_BYTES + (1 + slot) * Gm::PHI_BYTES);
+        const PT pL = W ? PC::from_d(s.phiW[rc]) : row[Gm::ALP + tid - 1];
+        const PT pM = row[Gm::ALP + tid];
+        const PT pR = E ? PC::from_d(s.phiE[rc]) : row[Gm::ALP + tid + 1];
+        const PA a0 = h * PC::onep(pL), a1 = h * PC::onep(pM), a2 = h * PC::onep(pR);
+        const PA b0 = h * PC::onem(pL), b1 = h * PC::onem(pM), b2 = h * PC::onem(pR);
+        ap[slot] = a0 * a0 + a1 * a1 + a2 * a2;
+        am[slot] = b0 * b0 + b1 * b1 + b2 * b2;
+        pc[slot] = pM;
+    }
+}
+
 /* lp_row: node (x, y) from a filled stage: the window's new row y+1, the
  * pulls (bounce-back and boundary values from global memory), node_lp, and
  * the window shift. */
@@ -687,9 +713,15 @@ flow_pipe_lp_kernel(LpPtrs<S, PT> s0, LpPtrs<S, PT> s1, ConstsLP<AT> c, PipeSche
         if (lane != 0) return;
         long long r = 0;
         bool bad = false;
+        /* the next ticket is claimed one tile ahead, so its round trip
+         * overlaps the current tile's copies; a claimed ticket is always
+         * larger than the one in progress, so the schedule stays free of
+         * deadlock */
+        unsigned long long next = atomicAdd(fl.ticket, 1ull);
         while (!bad) {
-            const unsigned long long item = atomicAdd(fl.ticket, 1ull);
+            const unsigned long long item = next;
             if (item >= (unsigned long long)total) break;
+            next = atomicAdd(fl.ticket, 1ull);
             const int k = (int)(item / sch.ntiles), t = (int)(item % sch.ntiles);
             if (k > 0 && !flow_deps(fl.done, t, sch, (unsigned)k, errflag)) {
                 atomicExch(errflag, 4);
@@ -707,8 +739,8 @@ flow_pipe_lp_kernel(LpPtrs<S, PT> s0, LpPtrs<S, PT> s1, ConstsLP<AT> c, PipeSche
                     break;
                 }
                 tag[st] = StageTag{k, t, y, (y == y0 ? TAG_FIRST : 0) | (y == y1 - 1 ? TAG_LAST : 0)};
-                pipe_issue<S, PT>(sk.fin, sk.gin, sk.phin, sk.plane, sk.P, Ny, x0, y,
-                                  stages + (size_t)st * Gm::STAGE_BYTES, &full[st]);
+                pipe_issue_w<S, PT>(sk.fin, sk.gin, sk.phin, sk.plane, sk.P, Ny, x0, y, y == y0,
+                                    stages + (size_t)st * Gm::STAGE_BYTES_W, &full[st]);
                 r++;
             }
         }
@@ -744,19 +776,23 @@ flow_pipe_lp_kernel(LpPtrs<S, PT> s0, LpPtrs<S, PT> s1, ConstsLP<AT> c, PipeSche
         const int x = (tg.t % sch.nbands) * sch.bx + tid;
         const bool W = (x == 0), E = (x == Nx - 1);
         if (x < Nx) {
-            if (tg.flags & TAG_FIRST) lp_window_start(sk, c, x, tg.y, W, E, ap, am, pc);
-            lp_row<S, PT, AT, TANH, false>(sk, c, stages + (size_t)st * Gm::STAGE_BYTES, x, tg.y, tid, W, E, ap, am,
-                                           pc);
+            const unsigned char *stg = stages + (size_t)st * Gm::STAGE_BYTES_W;
+            if (tg.flags & TAG_FIRST) lp_window_stage(sk, c, tg.y, tid, W, E, stg, ap, am, pc);
+            lp_row<S, PT, AT, TANH, false>(sk, c, stg, x, tg.y, tid, W, E, ap, am, pc);
         }
         if (tg.flags & TAG_LAST) {
-            /* this warp's part of the tile is stored; the last of the four
-             * warps publishes the tile's step */
-            __threadfence();
+            /* this warp's part of the tile is stored: the warp barrier orders
+             * the lanes' stores before lane 0's fence, whose cumulativity
+             * makes them visible device-wide (the pattern of a grid-wide
+             * barrier); the last of the four warps publishes the tile's step */
             __syncwarp();
-            if (lane == 0 && atomicAdd(&warps_done[st], 1) == PIPE_CWARPS - 1) {
-                warps_done[st] = 0;
+            if (lane == 0) {
                 __threadfence();
-                st_release_u32(fl.done + tg.t, (unsigned)tg.k + 1);
+                if (atomicAdd(&warps_done[st], 1) == PIPE_CWARPS - 1) {
+                    warps_done[st] = 0;
+                    __threadfence();
+                    st_release_u32(fl.done + tg.t, (unsigned)tg.k + 1);
+                }
             }
         }
         __syncwarp();
@@ -982,7 +1018,7 @@ cudaError_t launch_flow_t(bgk_ctx *c, int nsteps)
     fl.done = (unsigned *)((char *)c->flow_buf + sizeof(unsigned long long));
     fl.nsteps = nsteps;
     using Gm = PipeGeom<S, PT>;
-    const size_t smem = Gm::smem_bytes(D);
+    const size_t smem = Gm::smem_bytes_w(D);
     if (c->opt.tanh_mode == BGK_TANH_PORTABLE) {
         static std::atomic<unsigned long long> done{0};
         if ((e = pipe_configure(flow_pipe_lp_kernel<S, PT, AT, D, BGK_TANH_PORTABLE>, smem, c->dev, done))) return e;

@@ -183,8 +183,9 @@ inline cudaError_t pdl_launch(void (*kernel)(KArgs...), int grid, int block, siz
  * so the smallest unfinished ticket can always proceed and the schedule
  * needs no co-residency.
  *
- * Ordering: the consumers' stores of a tile are fenced (membar.gl) before
- * the last of its four warps releases done[t]; a producer acquires the
+ * Ordering: each consumer warp's stores of a tile are fenced (a warp
+ * barrier, then membar.gl by one lane) before the last of its four warps
+ * releases done[t]; a producer acquires the
  * flags, then orders the bulk copies (async proxy) after that with
  * fence.proxy.async, and hands the stage to its consumers through the
  * stage's mbarrier.  Every wait is bounded; on expiry the error flag is set
@@ -213,24 +214,47 @@ __device__ __forceinline__ void st_release_u32(unsigned *p, unsigned v)
 __device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
 
 /* Wait (bounded) until every tile of the 3x3 neighbourhood of t has done
- * `need` steps; false on expiry or once another CTA raised the error flag. */
+ * `need` steps; false on expiry or once another CTA raised the error flag.
+ * The nine counts are read together (relaxed, one round trip to L2 per
+ * poll); once all suffice, an acquire fence orders what follows after the
+ * stores that the counts publish. */
+__device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void fence_acquire_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
 __device__ bool flow_deps(const unsigned *done, int t, const PipeSched &sch, unsigned need, const int *errflag)
 {
     const int b = t % sch.nbands, st = t / sch.nbands;
+    const unsigned *p[9];
+    int n = 0;
     for (int ds = -1; ds <= 1; ds++) {
         const int ss = st + ds;
         if (ss < 0 || ss >= sch.nstrips) continue;
         for (int db = -1; db <= 1; db++) {
             const int bb = b + db;
             if (bb < 0 || bb >= sch.nbands) continue;
-            const unsigned *p = done + (long long)ss * sch.nbands + bb;
-            for (long long i = 0; ld_acquire_u32(p) < need; i++) {
-                if (i > PIPE_WAIT_LIMIT) return false;
-                if ((i & 255) == 255 && *(volatile const int *)errflag) return false;
-                if (i > 32) __nanosleep(64);
-            }
+            p[n++] = done + (long long)ss * sch.nbands + bb;
         }
     }
+    for (long long i = 0;; i++) {
+        unsigned v[9];
+#pragma unroll
+        for (int q = 0; q < 9; q++)
+            if (q < n) v[q] = ld_relaxed_u32(p[q]);
+        bool ok = true;
+#pragma unroll
+        for (int q = 0; q < 9; q++)
+            if (q < n && v[q] < need) ok = false;
+        if (ok) break;
+        if (i > PIPE_WAIT_LIMIT) return false;
+        if ((i & 255) == 255 && *(volatile const int *)errflag) return false;
+        if (i > 32) __nanosleep(64);
+    }
+    fence_acquire_gpu();
     return true;
 }
 

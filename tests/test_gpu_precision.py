@@ -51,9 +51,10 @@ def test_fp32_form_256_cavity_20k_steps(lib):
     rest populations closed each node's mass and energy, the FP32 form's
     collision rounding acted as a steady heat sink here: T was off by 1.7e-4
     dT and phi by 2.6e-3, the front lagging in every row.  Measured now:
-    T 6.8e-7 and phi 7.4e-6 against FP64 in double; 1.2e-5 and 9.7e-5
-    against the reference's rounding, whose own REAL(4) temporaries move phi
-    by 9.8e-5 on this case."""
+    T 6.9e-7 and phi 7.2e-6 against FP64 in double.  Against the
+    reference's rounding T 1.2e-5 and phi 1.0e-4: the reference's own REAL(4)
+    collision temporaries move its phi by 9.8e-5 from FP64 in double on this
+    case, so that comparison is bounded at twice the spread."""
     from bgk_pcm_b200 import inputs
     p = inputs.workload_params(**inputs.WORKLOADS["cavity256_ra1e5"])
     smooth = run("f64", p, 20000, smooth=True)
@@ -61,8 +62,8 @@ def test_fp32_form_256_cavity_20k_steps(lib):
     lo = run("f32", p, 20000)
     es, er = errors(smooth, lo, p), errors(ref, lo, p)
     print("fp32 vs smooth", es, "vs reference rounding", er)
-    assert es["T"] <= 1e-5 and es["phi"] <= 5e-5, es
-    assert er["T"] <= 1e-4 and er["phi"] <= 1e-4, er
+    assert es["T"] <= 5e-6 and es["phi"] <= 3e-5, es
+    assert er["T"] <= 1e-4 and er["phi"] <= 2e-4, er
 
 
 def test_fp32_form_mass_follows_fp64(lib):
@@ -164,3 +165,35 @@ def test_dataflow_steps_bit_identical(lib, monkeypatch, precision, phi64, Nx, Ny
             outs.append({n: s.field(n) for n in ("rho", "T", "u", "v", "phi", "phi_prec", "f3", "g7")})
     for n in outs[0]:
         np.testing.assert_array_equal(outs[1][n], outs[0][n], err_msg=n)
+
+
+def test_fp32_form_on_the_precision_workload(lib):
+    """The 4096^2, Ra 1e7 precision workload over its full 20,000 steps: the
+    FP32 form against the FP64 path (double throughout), max relative error
+    on T (by T0 - T_in_sol) and phi (by 2) <= 1e-4 at 5k, 10k and 20k steps.
+    Before the collision corrected the first-moment scaling of the rounded
+    float weights, phi was off by 5.1e-4 at 10k steps (the velocity drifted
+    by 6.5e-5 of max |u|); measured now: T 4.1e-5, phi 6.0e-5 at worst.
+    Against the reference's own rounding (REAL(4) collision temporaries) T
+    differs by 2.9e-4, the spread of those temporaries themselves."""
+    from bgk_pcm_b200 import Solver, inputs, precision
+    p = inputs.workload_params(**inputs.WORKLOADS["cavity4096_ra1e7"])
+    marks = (5000, 10000, 20000)
+
+    def run(**kw):
+        out, done = {}, 0
+        with Solver(p, **kw) as s:
+            s.initialization()
+            for m in marks:
+                s.step(m - done)
+                done = m
+                out[m] = {n: s.field(n)[1:-1, 1:-1].copy() for n in ("T", "phi", "u", "v")}
+        return out
+
+    ref = run(precision="f64", smooth=True)
+    lo = run(precision="f32")
+    for m in marks:
+        e = precision.errors(lo[m], ref[m], p)
+        print(f"step {m}: T {e['T_max']:.2e}  phi {e['phi_max']:.2e}  u {e['u_max']:.2e}  "
+              f"front dx mid/max {e['front_dx_mid_cells']} / {e['front_dx_max_cells']}")
+        assert e["T_max"] <= 1e-4 and e["phi_max"] <= 1e-4, (m, e)
