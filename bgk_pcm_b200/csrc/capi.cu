@@ -561,12 +561,19 @@ int bgk_step(bgk_ctx *c, int nsteps)
     const bool exact = f64 && !c->opt.fma;
     int t = 0;
     if (c->tune_flow && !c->ring && nsteps > 2) {
-        /* the steps before the two that write the moments, in one launch */
-        if (exact) CK(bgk::launch_flow_f64(c, nsteps - 2), "dataflow steps");
-        else CK(bgk::launch_flow_fast(c, nsteps - 2), "dataflow steps");
-        c->cur ^= (nsteps - 2) & 1;
-        c->it += nsteps - 2;
-        t = nsteps - 2;
+        /* the steps before the two that write the moments in one launch
+         * (BGK_FLOW=1), or in one launch each with tiles handed out on
+         * demand (BGK_FLOW=2) */
+        const int nflow = nsteps - 2;
+        for (int done = 0; done < nflow;) {
+            const int n = c->tune_flow == 2 ? 1 : nflow;
+            if (exact) CK(bgk::launch_flow_f64(c, n), "dataflow steps");
+            else CK(bgk::launch_flow_fast(c, n), "dataflow steps");
+            c->cur ^= n & 1;
+            c->it += n;
+            done += n;
+        }
+        t = nflow;
     }
     for (; t < nsteps; t++) {
         const bool last = (t == nsteps - 1);
