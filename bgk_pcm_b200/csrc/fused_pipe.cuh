@@ -354,11 +354,16 @@ flow_pipe_f64_kernel(StepPtrs<double> s0, StepPtrs<double> s1, Consts c, const d
             if (item >= (unsigned long long)total) break;
             next = atomicAdd(fl.ticket, 1ull);
             const int k = (int)(item / sch.ntiles), t = (int)(item % sch.ntiles);
-            if (k > 0 && !flow_deps(fl.done, t, sch, (unsigned)k, errflag)) {
-                atomicExch(errflag, 4);
-                break;
+            if (k > 0) {
+                /* items of the first step read what earlier launches wrote
+                 * (ordered by the launch boundary); later ones read other
+                 * CTAs' stores of this launch through the bulk copies */
+                if (!flow_deps(fl.done, t, sch, (unsigned)k, errflag)) {
+                    atomicExch(errflag, 4);
+                    break;
+                }
+                fence_proxy_async_global();
             }
-            fence_proxy_async_global();
             const StepPtrs<double> &sk = (k & 1) ? s1 : s0;
             const int x0 = (t % sch.nbands) * sch.bx, y0 = (t / sch.nbands) * sch.H;
             const int y1 = min(y0 + sch.H, Ny);
