@@ -161,6 +161,8 @@ struct bgk_ctx {
     int tune_flow;         /* 1: reduced-precision steps between outputs in one
                             * dataflow launch (BGK_FLOW)                    */
     void *flow_buf;        /* its ticket counter and per-tile step counts   */
+    int flow_stall;        /* test of the error path: dependency waits of a
+                            * dataflow launch never succeed (BGK_FLOW_STALL) */
     size_t flow_bytes;
     void *adj_ws;          /* adjoint workspace kept between bgk_adjoint_run calls */
     size_t adj_ws_bytes;

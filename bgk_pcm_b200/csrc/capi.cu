@@ -442,6 +442,8 @@ int bgk_create(const bgk_params *pp, const bgk_options *opt, bgk_ctx **out)
     if (const char *v = getenv("BGK_PIPE_CTAS")) c->tune_ctas = atoi(v);
     c->tune_flow = 0;
     if (const char *v = getenv("BGK_FLOW")) c->tune_flow = atoi(v);
+    c->flow_stall = 0;
+    if (const char *v = getenv("BGK_FLOW_STALL")) c->flow_stall = atoi(v) == 1;
     {
         cudaDeviceProp pr;
         c->nsm = (cudaGetDeviceProperties(&pr, dev) == cudaSuccess) ? pr.multiProcessorCount : 148;

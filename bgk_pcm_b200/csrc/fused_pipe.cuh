@@ -358,7 +358,7 @@ flow_pipe_f64_kernel(StepPtrs<double> s0, StepPtrs<double> s1, Consts c, const d
                 /* items of the first step read what earlier launches wrote
                  * (ordered by the launch boundary); later ones read other
                  * CTAs' stores of this launch through the bulk copies */
-                if (!flow_deps(fl.done, t, sch, (unsigned)k, errflag)) {
+                if (!flow_deps(fl.done, t, sch, (unsigned)k + fl.stall, errflag)) {
                     atomicExch(errflag, 4);
                     break;
                 }
@@ -460,6 +460,7 @@ inline cudaError_t flow_f64_launch_t(bgk_ctx *c, const StepPtrs<double> &s0, con
     fl.ticket = (unsigned long long *)c->flow_buf;
     fl.done = (unsigned *)((char *)c->flow_buf + sizeof(unsigned long long));
     fl.nsteps = nsteps;
+    fl.stall = c->flow_stall ? (1u << 30) : 0u;
     flow_pipe_f64_kernel<D, T, R><<<grid, PIPE_THREADS, smem, c->stream>>>(s0, s1, c->c, c->corner, sch, fl,
                                                                           c->errflag);
     return cudaGetLastError();

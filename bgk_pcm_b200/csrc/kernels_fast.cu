@@ -727,7 +727,7 @@ flow_pipe_lp_kernel(LpPtrs<S, PT> s0, LpPtrs<S, PT> s1, ConstsLP<AT> c, PipeSche
                 /* items of the first step read what earlier launches wrote
                  * (ordered by the launch boundary); later ones read other
                  * CTAs' stores of this launch through the bulk copies */
-                if (!flow_deps(fl.done, t, sch, (unsigned)k, errflag)) {
+                if (!flow_deps(fl.done, t, sch, (unsigned)k + fl.stall, errflag)) {
                     atomicExch(errflag, 4);
                     break;
                 }
@@ -1022,6 +1022,7 @@ cudaError_t launch_flow_t(bgk_ctx *c, int nsteps)
     fl.ticket = (unsigned long long *)c->flow_buf;
     fl.done = (unsigned *)((char *)c->flow_buf + sizeof(unsigned long long));
     fl.nsteps = nsteps;
+    fl.stall = c->flow_stall ? (1u << 30) : 0u;
     using Gm = PipeGeom<S, PT>;
     const size_t smem = Gm::smem_bytes_w(D);
     if (c->opt.tanh_mode == BGK_TANH_PORTABLE) {

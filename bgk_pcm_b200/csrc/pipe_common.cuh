@@ -56,12 +56,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
-/* Bounded wait: false after ~PIPE_WAIT_LIMIT polls. */
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+/* Bounded wait: false after ~PIPE_WAIT_LIMIT polls or about a second of
+ * wall clock, whichever comes first (a try_wait may itself suspend the
+ * thread for a while before it reports an incomplete phase). */
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
 {
+    unsigned long long t0 = 0;
     for (long long i = 0; i < PIPE_WAIT_LIMIT; i++) {
         if (mbar_try_wait(bar, parity)) return true;
         if (i > 32) __nanosleep(64);
+        if (i == 1024) t0 = global_ns();
+        if (i > 1024 && (i & 1023) == 0 && global_ns() - t0 > 1000000000ull) return false;
     }
     return false;
 }
@@ -195,6 +207,8 @@ struct FlowCtl {
     unsigned long long *ticket; /* next work item (zero at launch)         */
     unsigned *done;     /* [ntiles]: steps completed by each tile (zero)   */
     int nsteps;
+    unsigned stall;     /* added to every dependency target: 0, or (to test
+                         * the error path) a count no tile reaches        */
 };
 struct StageTag {
     int k, t, y, flags;
@@ -240,6 +254,7 @@ __device__ bool flow_deps(const unsigned *done, int t, const PipeSched &sch, uns
             p[n++] = done + (long long)ss * sch.nbands + bb;
         }
     }
+    const unsigned long long t0 = global_ns();
     for (long long i = 0;; i++) {
         unsigned v[9];
 #pragma unroll
@@ -251,7 +266,7 @@ __device__ bool flow_deps(const unsigned *done, int t, const PipeSched &sch, uns
             if (q < n && v[q] < need) ok = false;
         if (ok) break;
         if (i > PIPE_WAIT_LIMIT) return false;
-        if ((i & 255) == 255 && *(volatile const int *)errflag) return false;
+        if ((i & 255) == 255 && (*(volatile const int *)errflag || global_ns() - t0 > 1000000000ull)) return false;
         if (i > 32) __nanosleep(64);
     }
     fence_acquire_gpu();
