@@ -414,7 +414,7 @@ flow_pipe_f64_kernel(StepPtrs<double> s0, StepPtrs<double> s1, Consts c, const d
             if (tg.flags & TAG_FIRST) f64_window_stage(sk, Ny, tg.y, tid, W, E, stg, ap, am, pc);
             f64_row<TANH, false, REF32, false>(sk, c, corner, stg, x, tg.y, tid, W, E, ap, am, pc);
         }
-        if (tg.flags & TAG_LAST) {
+        if ((tg.flags & TAG_LAST) && fl.nsteps > 1) {
             /* this warp's part of the tile is stored: the warp barrier orders
              * the lanes' stores before lane 0's fence, whose cumulativity
              * makes them visible device-wide (the pattern of a grid-wide

@@ -785,7 +785,7 @@ flow_pipe_lp_kernel(LpPtrs<S, PT> s0, LpPtrs<S, PT> s1, ConstsLP<AT> c, PipeSche
             if (tg.flags & TAG_FIRST) lp_window_stage(sk, c, tg.y, tid, W, E, stg, ap, am, pc);
             lp_row<S, PT, AT, TANH, false>(sk, c, stg, x, tg.y, tid, W, E, ap, am, pc);
         }
-        if (tg.flags & TAG_LAST) {
+        if ((tg.flags & TAG_LAST) && fl.nsteps > 1) {
             /* this warp's part of the tile is stored: the warp barrier orders
              * the lanes' stores before lane 0's fence, whose cumulativity
              * makes them visible device-wide (the pattern of a grid-wide

@@ -197,7 +197,7 @@ inline cudaError_t pdl_launch(void (*kernel)(KArgs...), int grid, int block, siz
  *
  * Ordering: each consumer warp's stores of a tile are fenced (a warp
  * barrier, then membar.gl by one lane) before the last of its four warps
- * releases done[t]; a producer acquires the
+ * releases done[t] (a one-step launch has no readers and skips this); a producer acquires the
  * flags, then orders the bulk copies (async proxy) after that with
  * fence.proxy.async, and hands the stage to its consumers through the
  * stage's mbarrier.  Every wait is bounded; on expiry the error flag is set
