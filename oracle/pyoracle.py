@@ -62,13 +62,14 @@ def load() -> ctypes.CDLL:
     lib.orc_step.argtypes = [vp, ctypes.c_int]
     lib.orc_set_tanh_mode.argtypes = [vp, ctypes.c_int]
     lib.orc_set_smooth.argtypes = [vp, ctypes.c_int]
+    lib.orc_set_heat.argtypes = [vp, ctypes.c_int]
     lib.orc_set_threads.argtypes = [ctypes.c_int]
     lib.orc_get_it.argtypes = [vp]
     lib.orc_set_it.argtypes = [vp, ctypes.c_int]
     lib.orc_sums.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     lib.orc_open_outputs.argtypes = [vp, ctypes.c_char_p]
     lib.orc_read_input.argtypes = [ctypes.c_char_p, ctypes.POINTER(OrcParams)]
-    lib.orc_main.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
+    lib.orc_main.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     lib.orc_portable_tanh.restype = ctypes.c_double
     lib.orc_portable_tanh.argtypes = [ctypes.c_double]
     dp = ctypes.POINTER(ctypes.c_double)
@@ -93,7 +94,7 @@ class Oracle:
 
     STAGES = ("bc_f", "bc_g", "streaming", "moments_pre", "phase_field", "forces", "collision", "moments")
 
-    def __init__(self, params: dict, tanh: str = "libm", threads: int = 0, smooth: bool = False):
+    def __init__(self, params: dict, tanh: str = "libm", threads: int = 0, smooth: bool = False, heat: int = 0):
         self.lib = load()
         p = OrcParams()
         for n, _ in OrcParams._fields_:
@@ -106,6 +107,8 @@ class Oracle:
             raise ValueError("orc_create failed")
         self.lib.orc_set_tanh_mode(self.h, 1 if tanh == "portable" else 0)
         self.lib.orc_set_smooth(self.h, 1 if smooth else 0)
+        # STEP_DOCONCURRENT's heating options: 1 FROMRIGHT, 2 FROMBOTTOM, 3 both
+        self.lib.orc_set_heat(self.h, int(heat))
 
     def close(self):
         if self.h:
@@ -153,11 +156,12 @@ def portable_tanh(x: float) -> float:
     return load().orc_portable_tanh(float(x))
 
 
-def run_main(workdir, threads: int = 0, tanh_mode: int = 0) -> None:
+def run_main(workdir, threads: int = 0, tanh_mode: int = 0, heat: int = 0) -> None:
     """Run the STEP_7 program (orc_main) in workdir (must hold input.dat)."""
     if not MAIN.exists():
         build()
-    r = subprocess.run([str(MAIN), str(workdir), str(threads), str(tanh_mode)], capture_output=True, text=True)
+    r = subprocess.run([str(MAIN), str(workdir), str(threads), str(tanh_mode), str(heat)], capture_output=True,
+                       text=True)
     if r.returncode != 0:
         raise RuntimeError(r.stderr)
 

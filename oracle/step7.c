@@ -63,6 +63,7 @@ struct orc_state {
     int deltaOut, itOut;
     int tanh_mode;
     int smooth;            /* 1: keep ft/gt in double (the differentiable form) */
+    int heat;              /* ORC_HEAT_* bits (STEP_DOCONCURRENT's FROMRIGHT / FROMBOTTOM) */
     /* diag.f90's melt_front/melt_front_expected are locals that are not
      * assigned on every path; they are carried from call to call here. */
     double diag_melt_front, diag_melt_front_expected;
@@ -224,6 +225,7 @@ void orc_destroy(orc_state *s)
 
 void orc_set_tanh_mode(orc_state *s, int mode) { s->tanh_mode = mode; }
 void orc_set_smooth(orc_state *s, int smooth) { s->smooth = smooth; }
+void orc_set_heat(orc_state *s, int heat) { s->heat = heat; }
 double *orc_field(orc_state *s, int id) { return (id >= 0 && id < ORC_NFIELDS) ? s->fld[id] : NULL; }
 int orc_get_it(const orc_state *s) { return s->it; }
 void orc_set_it(orc_state *s, int it) { s->it = it; }
@@ -250,26 +252,27 @@ static inline void feq9(const double *w, double r, double u, double v, double *e
 
 /* ------------------------------------------------------- initialization */
 
-/* STEP_7/initialization.f90:5-152 */
+/* STEP_7/initialization.f90:5-152; with heat bits, the branches of
+ * STEP_DOCONCURRENT/initialization.f90:16-62 (T/rho), :122-137 (T buffer)
+ * and :208-222 (phi). */
 void orc_initialization(orc_state *s)
 {
     const int Nx = s->Nx, Ny = s->Ny;
+    const int right = s->heat & ORC_HEAT_RIGHT, bottom = s->heat & ORC_HEAT_BOTTOM;
     s->interf = Nx / 40;
     s->Tin = s->T0;
     s->u0 = s->Re * s->kvisc / s->length;
     s->v0 = 0.0;
     s->Mach = s->u0 / s->cs;
 
-    for (int j = 0; j <= Ny + 1; j++) {
-        for (int i = 0; i <= s->interf; i++) {
-            TT[IX(i, j)] = s->T0;
-            RHO[IX(i, j)] = s->rho1;
+    for (int j = 0; j <= Ny + 1; j++)
+        for (int i = 0; i <= Nx + 1; i++) {
+            /* liquid layer: rows 0..interf (FROMBOTTOM; interf = Nx/40 also
+             * here), columns Nx-interf+1..Nx+1 (FROMRIGHT) or 0..interf */
+            const int liquid = bottom ? (j <= s->interf) : right ? (i >= Nx - s->interf + 1) : (i <= s->interf);
+            TT[IX(i, j)] = liquid ? s->T0 : s->T_in_sol;
+            RHO[IX(i, j)] = liquid ? s->rho1 : s->rho0;
         }
-        for (int i = s->interf + 1; i <= Nx + 1; i++) {
-            TT[IX(i, j)] = s->T_in_sol;
-            RHO[IX(i, j)] = s->rho0;
-        }
-    }
     for (size_t q = 0; q < s->A; q++) { UU[q] = s->u0; VV[q] = s->v0; }
 
     static const double cx[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
@@ -277,7 +280,16 @@ void orc_initialization(orc_state *s)
     memcpy(s->cx, cx, sizeof cx);
     memcpy(s->cy, cy, sizeof cy);
 
-    for (int j = 0; j <= Ny + 1; j++) TT[IX(0, j)] = s->Tin;
+    if (bottom) {
+        /* `do i = 0,Ny+1; T(i,0) = Tin`: the index runs to Ny+1 along x, so
+         * with Ny > Nx it continues past the end of row 0 into row 1 (column-
+         * major storage, no bounds check): the first Ny+2 cells in memory */
+        for (int i = 0; i <= Ny + 1; i++) TT[i] = s->Tin;
+    } else if (right) {
+        for (int j = 0; j <= Ny + 1; j++) TT[IX(Nx + 1, j)] = s->Tin;
+    } else {
+        for (int j = 0; j <= Ny + 1; j++) TT[IX(0, j)] = s->Tin;
+    }
     for (int i = 0; i <= Nx + 1; i++) {
         UU[IX(i, Ny + 1)] = 0.0; VV[IX(i, Ny + 1)] = 0.0;
         UU[IX(i, 0)] = 0.0; VV[IX(i, 0)] = 0.0;
@@ -306,8 +318,11 @@ void orc_initialization(orc_state *s)
             for (int k = 0; k < 9; k++) G(k)[q] = e[k];
         }
     for (size_t q = 0; q < s->A; q++) { PHI[q] = -1.0; PHIP[q] = -1.0; }
+    /* FROMRIGHT's phi strip starts at Nx-interf, one column left of its T
+     * strip; FROMBOTTOM keeps the west phi strip */
+    const int p0 = right ? Nx - s->interf : 0, p1 = right ? Nx + 1 : s->interf;
     for (int j = 0; j <= Ny + 1; j++)
-        for (int i = 0; i <= s->interf; i++) {
+        for (int i = p0; i <= p1; i++) {
             PHI[IX(i, j)] = 1.0;
             PHIP[IX(i, j)] = 1.0;
         }
@@ -452,12 +467,38 @@ void orc_bc_f(orc_state *s)
 /* ----------------------------------------------------------------- BC_g */
 
 /* STEP_7/BC_g.f90:5-64 (no branches: W Dirichlet Tin, E zero-gradient T,
- * N/S copies of all nine g, T and phi). */
+ * N/S copies of all nine g, T and phi).  With ORC_HEAT_RIGHT, the FROMRIGHT
+ * branches of STEP_DOCONCURRENT/BC_g.f90:13-45: W zero-gradient T, whose g1,
+ * g5, g8 take the -x equilibrium polynomials of directions 3, 7, 6 (the
+ * sign flip is the reference's), E Dirichlet Tin.  DOCONCURRENT's loops run
+ * over j = 0..Ny / 0..Ny+1; rows 0 and Ny+1 are overwritten by the N/S copies
+ * below, so j = 1..Ny gives the same arrays. */
 void orc_bc_g(orc_state *s)
 {
     const int Nx = s->Nx, Ny = s->Ny;
     const double *w = s->w;
-    for (int j = 1; j <= Ny; j++) {
+    if (s->heat & ORC_HEAT_RIGHT) {
+        for (int j = 1; j <= Ny; j++) {
+            double u = UU[IX(0, j)], v = VV[IX(0, j)];
+            double uu = u * u, vv = v * v, uv = 1.5 * (uu + vv);
+            double upv = u + v, umv = u - v;
+            double t = TT[IX(1, j)];
+            G(1)[IX(0, j)] = w[1] * t * (1.0 - 3.0 * u + 4.5 * uu - uv);
+            G(5)[IX(0, j)] = w[5] * t * (1.0 - 3.0 * upv + 4.5 * upv * upv - uv);
+            G(8)[IX(0, j)] = w[8] * t * (1.0 - 3.0 * umv + 4.5 * umv * umv - uv);
+            TT[IX(0, j)] = TT[IX(1, j)];
+        }
+        for (int j = 1; j <= Ny; j++) {
+            double u = UU[IX(Nx + 1, j)], v = VV[IX(Nx + 1, j)];
+            double uu = u * u, vv = v * v, uv = 1.5 * (uu + vv);
+            double upv = u + v, umv = u - v;
+            G(3)[IX(Nx + 1, j)] = w[3] * s->Tin * (1.0 - 3.0 * u + 4.5 * uu - uv);
+            G(6)[IX(Nx + 1, j)] = w[6] * s->Tin * (1.0 - 3.0 * umv + 4.5 * umv * umv - uv);
+            G(7)[IX(Nx + 1, j)] = w[7] * s->Tin * (1.0 - 3.0 * upv + 4.5 * upv * upv - uv);
+            TT[IX(Nx + 1, j)] = s->Tin;
+        }
+    }
+    for (int j = 1; j <= Ny && !(s->heat & ORC_HEAT_RIGHT); j++) {
         double u = UU[IX(0, j)], v = VV[IX(0, j)];
         double uu = u * u, vv = v * v, uv = 1.5 * (uu + vv);
         double upv = u + v, umv = u - v;
@@ -466,7 +507,7 @@ void orc_bc_g(orc_state *s)
         G(8)[IX(0, j)] = w[8] * s->Tin * (1.0 + 3.0 * umv + 4.5 * umv * umv - uv);
         TT[IX(0, j)] = s->Tin;
     }
-    for (int j = 1; j <= Ny; j++) {
+    for (int j = 1; j <= Ny && !(s->heat & ORC_HEAT_RIGHT); j++) {
         double u = UU[IX(Nx + 1, j)], v = VV[IX(Nx + 1, j)];
         double uu = u * u, vv = v * v, uv = 1.5 * (uu + vv);
         double upv = u + v, umv = u - v;
@@ -987,7 +1028,7 @@ void orc_out2d(orc_state *s)
 
 /* STEP_7/main.f90:18-122 (restart path excluded: dump_out is commented out
  * in the reference and dump_in does not restore phi). */
-int orc_main(const char *dir, int nthreads, int tanh_mode)
+int orc_main(const char *dir, int nthreads, int tanh_mode, int heat)
 {
     char path[1200];
     snprintf(path, sizeof path, "%s/input.dat", dir);
@@ -997,6 +1038,7 @@ int orc_main(const char *dir, int nthreads, int tanh_mode)
     orc_state *s = orc_create(&p);
     if (!s) return -2;
     s->tanh_mode = tanh_mode;
+    s->heat = heat;
     if (orc_open_outputs(s, dir)) { orc_destroy(s); return -3; }
     snprintf(path, sizeof path, "%s/log.dat", dir);
     FILE *lg = fopen(path, "w");

@@ -60,6 +60,13 @@ void orc_set_tanh_mode(orc_state *s, int mode);
 /* 1 = keep collision.f90's ft/gt temporaries in double (the smooth,
  * differentiable form); 0 = their implicit REAL(4) (the reference). */
 void orc_set_smooth(orc_state *s, int smooth);
+/* Heated wall of STEP_DOCONCURRENT's preprocessor options, as bits:
+ * ORC_HEAT_RIGHT = FROMRIGHT (east wall at Tin, west wall zero-gradient,
+ * liquid strip on the east side), ORC_HEAT_BOTTOM = FROMBOTTOM (initial
+ * liquid layer along the south wall); 0 = STEP_7 (heated west wall).
+ * Both bits = both macros defined.  Set before orc_initialization. */
+enum { ORC_HEAT_RIGHT = 1, ORC_HEAT_BOTTOM = 2 };
+void orc_set_heat(orc_state *s, int heat);
 /* OpenMP threads for the hot loops (0 = leave the runtime default). */
 void orc_set_threads(int n);
 
@@ -99,7 +106,7 @@ void orc_sums(orc_state *s, double out[4]);
 
 /* The whole program of STEP_7/main.f90 run inside dir (reads dir/input.dat,
  * writes the reference's output files there).  Returns 0 on success. */
-int orc_main(const char *dir, int nthreads, int tanh_mode);
+int orc_main(const char *dir, int nthreads, int tanh_mode, int heat);
 
 /* bgk_portable_tanh, exported for the tests. */
 double orc_portable_tanh(double x);

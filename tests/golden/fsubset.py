@@ -21,6 +21,9 @@ declarations, allocate, DO loops, IF blocks, assignments (scalar, element and
 whole-array), CALL, and the intrinsics tanh, sqrt, acos, abs, int, float,
 real, dble, mod.  I/O statements are skipped except the list-directed reads of
 input.dat in setup, which take their values from a parameter dictionary.
+`do concurrent (i=a:b)` with one index (STEP_DOCONCURRENT's BC_g) runs as a
+sequential DO loop, which is one of the orders the construct allows; cpp
+conditionals are resolved against the macros a Program is given.
 """
 from __future__ import annotations
 
@@ -54,7 +57,7 @@ def _strip_comment(line: str) -> str:
 
 
 def preprocess(text: str, defined=()) -> list[str]:
-    """cpp conditionals (no macro defined), comments, continuations."""
+    """cpp conditionals (the macros in `defined`), comments, continuations."""
     lines, stack = [], []
     for raw in text.splitlines():
         s = raw.strip()
@@ -465,6 +468,9 @@ class Unit:
             return []
         if key.startswith("allocate"):
             return self.allocate(st, ind)
+        mc = re.match(r"^do concurrent\s*\(\s*(\w+)\s*=\s*([^:]+):([^:]+)\)$", key)
+        if mc:
+            key = f"do {mc.group(1)} = {mc.group(2)}, {mc.group(3)}"
         m = re.match(r"^do\s+(\w+)\s*=\s*(.+)$", key)
         if m:
             var = m.group(1)
@@ -685,8 +691,8 @@ def parse_module(path: Path):
     return module, init
 
 
-def subroutine_units(path: Path, module):
-    stmts = preprocess(path.read_text())
+def subroutine_units(path: Path, module, defined=()):
+    stmts = preprocess(path.read_text(), defined)
     units = []
     i = 0
     while i < len(stmts):
@@ -736,7 +742,9 @@ def fmod_(a, b):
 class Program:
     """The reference's STEP_7 subroutines, executable from Python."""
 
-    def __init__(self, ref_dir: Path, files):
+    def __init__(self, ref_dir: Path, files, defined=()):
+        """files: names in ref_dir, or paths (e.g. a sibling variant's file
+        that replaces one routine); defined: cpp macros."""
         self.module, init = parse_module(ref_dir / "shared.f90")
         src = [PRELUDE]
         for nm, typ, val in init:
@@ -760,7 +768,7 @@ class Program:
                 src.append(f"{nm} = {'0' if s.typ == 'i' else ('F32(0.0)' if s.typ == 'r4' else ('0.0' if s.typ == 'r8' else 'None'))}")
         self.units = {}
         for f in files:
-            for u in subroutine_units(ref_dir / f, self.module):
+            for u in subroutine_units(ref_dir / f, self.module, defined):
                 code = u.gen()
                 self.units[u.name] = code
                 src.append(code)

@@ -9,7 +9,8 @@ giving the root of the reference checkout (the directory holding STEP_7/):
 The STEP_7 routines (setup, initialization, BC_f, BC_g, streaming,
 momentsPre, phase_field, forces, collision, moments) are translated by
 fsubset.py and stepped in the order of STEP_7/main.f90's time loop, which is
-read from main.f90 itself.  After initialization, after the first step and
+read from main.f90 itself.  The heating-option cases take initialization and
+BC_g from STEP_DOCONCURRENT/ with its FROMRIGHT / FROMBOTTOM macros defined.  After initialization, after the first step and
 after the last step, all 46 module arrays are stored (float64, reference
 layout) in one .npz per case, together with the input parameters.
 """
@@ -51,6 +52,12 @@ def cavity(Nx, Ny, **kw):
     return d
 
 
+# STEP_DOCONCURRENT's heating options: preprocessor macros of its
+# initialization.f90 and BC_g.f90, which replace STEP_7's two routines (the
+# rest of the step is STEP_7's); bits as in the oracle's orc_set_heat
+HEAT_MACROS = {1: ("FROMRIGHT",), 2: ("FROMBOTTOM",), 3: ("FROMRIGHT", "FROMBOTTOM")}
+HEAT_FILES = ("initialization.f90", "BC_g.f90")
+
 # (name, params, steps): small grids the Python execution finishes in seconds
 CASES = [
     ("cavity_16x12", cavity(16, 12), 12),
@@ -61,6 +68,15 @@ CASES = [
     ("bc_periodic_inflow_9x8", cavity(9, 8, westBC=1, eastBC=3, northBC=6, southBC=6, Re=20.0), 5),
     ("bc_parabolic_sym_9x8", cavity(9, 8, westBC=2, eastBC=0, northBC=5, southBC=0, Re=20.0), 5),
     ("bc_pressure_9x8", cavity(9, 8, westBC=3, eastBC=4, northBC=1, southBC=4, Re=20.0), 5),
+    # heating options (params key "heat"): FROMRIGHT on the cavity; FROMRIGHT
+    # with a parabolic west inflow, where u(0,j) != 0 exposes the sign of the
+    # west g polynomials; FROMBOTTOM with Ny > Nx, where the T buffer loop runs
+    # past row 0; both macros; Nx >= 40 so that the liquid strip is wider
+    # than the wall column
+    ("heat_right_44x10", cavity(44, 10, heat=1), 8),
+    ("heat_right_inflow_9x8", cavity(9, 8, westBC=2, eastBC=0, northBC=4, southBC=4, Re=20.0, heat=1), 6),
+    ("heat_bottom_10x14", cavity(10, 14, heat=2), 6),
+    ("heat_right_bottom_41x9", cavity(41, 9, heat=3), 6),
 ]
 
 
@@ -82,7 +98,9 @@ def main_loop_order(ref: Path) -> list[str]:
 
 
 def run_case(ref: Path, params: dict, steps: int, order):
-    prog = fsubset.Program(ref / "STEP_7", FILES)
+    heat = params.get("heat", 0)
+    files = [ref / "STEP_DOCONCURRENT" / f if heat and f in HEAT_FILES else f for f in FILES]
+    prog = fsubset.Program(ref / "STEP_7", files, defined=HEAT_MACROS.get(heat, ()))
     p = {}
     for nm in INPUT_NAMES:
         key = nm.replace("_st", "") if nm.endswith("_st") else nm
@@ -106,13 +124,18 @@ def main():
     import argparse
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("reference", type=Path, help="root of the reference checkout (the directory holding STEP_7/)")
-    ref = ap.parse_args().reference
+    ap.add_argument("--only", default="", help="comma list of case names to regenerate (default: all)")
+    a = ap.parse_args()
+    ref = a.reference
     if not (ref / "STEP_7" / "main.f90").is_file():
         ap.error(f"{ref}/STEP_7/main.f90 not found")
     order = main_loop_order(ref)
     assert order == ["bc_f", "bc_g", "streaming", "momentspre", "phase_field", "forces", "collision",
                      "moments"], order
+    only = set(a.only.split(",")) if a.only else None
     for name, params, steps in CASES:
+        if only and name not in only:
+            continue
         t0 = time.time()
         snaps = run_case(ref, params, steps, order)
         arrays = {f"{tag}/{f}": a for tag, d in snaps.items() for f, a in d.items()}
