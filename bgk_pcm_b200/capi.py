@@ -26,6 +26,7 @@ ERRORS = {
 
 PREC_F64, PREC_F32, PREC_F16, PREC_F32X = 0, 1, 2, 3
 TANH_PORTABLE, TANH_DEVICE = 0, 1
+HEAT_WEST, HEAT_RIGHT, HEAT_BOTTOM = 0, 1, 2
 
 FIELD_F0, FIELD_G0 = 0, 9
 FIELD_RHO, FIELD_T, FIELD_U, FIELD_V = 18, 19, 20, 21
@@ -78,7 +79,7 @@ class Params(ctypes.Structure):
 
 class Options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("tanh_mode", ctypes.c_int), ("fma", ctypes.c_int),
-                ("device", ctypes.c_int), ("smooth", ctypes.c_int)]
+                ("device", ctypes.c_int), ("smooth", ctypes.c_int), ("heat", ctypes.c_int)]
 
 
 class AdjointSpec(ctypes.Structure):

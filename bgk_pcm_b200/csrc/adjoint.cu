@@ -811,7 +811,7 @@ adj_pipe_kernel(AdjPtrs s, Consts c, PipeSched sch, int *errflag)
  * times (H + 1), the 1 standing for the per-tile window prologue. */
 PipeSched adj_sched(const bgk_ctx *c, int ctas_per_sm, int bx, int *grid)
 {
-    PipeSched sch;
+    PipeSched sch{};   /* tiles of H rows (ranges = 0): the wall tables hold one tile */
     sch.bx = bx;
     sch.nbands = (c->Nx + bx - 1) / bx;
     const long long slots = (long long)c->nsm * ctas_per_sm;

@@ -63,6 +63,7 @@ struct Consts {
     double u0, v0;         /* initialization.f90:11-12                      */
     double rho0, rho1, T0, T_in_sol;
     int interf;            /* initialization.f90:5                           */
+    int heat;              /* BGK_HEAT_* bits (STEP_DOCONCURRENT's options)  */
 };
 
 /* Device pointers of one fused step. Ref-layout mirrors use pitch NX2. */
@@ -128,6 +129,8 @@ struct bgk_ctx {
     double *tcol[2];
     double *gW, *pE, *phiW, *phiE;
     double *tin_rows;      /* device [Ny] or null                           */
+    double *tright;        /* BGK_HEAT_RIGHT: [Ny] of Tin, the east wall's T  */
+                           /* column in place of the lagged T(Nx,j)          */
     double *tin_host;      /* host copy [Ny] or null                        */
     bool bc_dirty;
     bgk::LowpScale scale;
@@ -158,6 +161,8 @@ struct bgk_ctx {
      * pulls; pipeline depth and CTAs per SM (BGK_PIPE, BGK_PIPE_D,
      * BGK_PIPE_CTAS) */
     int tune_pipe, tune_D, tune_ctas, nsm;
+    int tune_sched;        /* per-step pipeline schedule: 0 tiles, 1 equal row
+                            * ranges (BGK_SCHED)                            */
     int tune_flow;         /* 1: reduced-precision steps between outputs in one
                             * dataflow launch (BGK_FLOW)                    */
     void *flow_buf;        /* its ticket counter and per-tile step counts   */
@@ -171,6 +176,10 @@ struct bgk_ctx {
 namespace bgk {
 
 /* kernels_f64.cu (compiled with --fmad=false: the reference's roundings) */
+/* T column the step's east g halos use: T(Nx,j) of the previous step
+ * (tcol[buf]), or the constant Tin column with BGK_HEAT_RIGHT */
+inline const double *east_tcol(const bgk_ctx *c, int buf) { return c->tright ? c->tright : c->tcol[buf]; }
+
 cudaError_t launch_init_f64(bgk_ctx *c);
 cudaError_t launch_bc_prep(bgk_ctx *c);
 cudaError_t launch_ring_bc(bgk_ctx *c);            /* BC_f + BC_g halos, walls other than 4 */

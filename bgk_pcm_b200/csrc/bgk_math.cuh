@@ -20,6 +20,36 @@
 
 namespace bgk {
 
+/* The initial condition of cell (i,j), 0 <= i <= Nx+1, 0 <= j <= Ny+1:
+ * STEP_7/initialization.f90:15-26,45-47,137-151, with the heat bits selecting
+ * the FROMRIGHT / FROMBOTTOM branches of STEP_DOCONCURRENT/initialization.f90
+ * (:16-62 the liquid layer of T and rho, :122-137 the T buffer, :208-222 the
+ * phi strip).  FROMBOTTOM's T buffer loop `do i = 0,Ny+1; T(i,0) = Tin` runs
+ * along x and, with Ny > Nx, continues into row 1 of the column-major
+ * array: it covers the first Ny+2 cells in memory. */
+BGK_HD bool init_liquid(const Consts &c, int i, int j)
+{
+    if (c.heat & BGK_HEAT_BOTTOM) return j <= c.interf;
+    if (c.heat & BGK_HEAT_RIGHT) return i >= c.Nx - c.interf + 1;
+    return i <= c.interf;
+}
+
+BGK_HD double init_T(const Consts &c, int i, int j)
+{
+    const long long q = (long long)i + (long long)(c.Nx + 2) * j;
+    const bool buffer = (c.heat & BGK_HEAT_BOTTOM) ? q <= (long long)c.Ny + 1
+                      : (c.heat & BGK_HEAT_RIGHT) ? i == c.Nx + 1 : i == 0;
+    return buffer ? c.Tin : (init_liquid(c, i, j) ? c.T0 : c.T_in_sol);
+}
+
+BGK_HD double init_rho(const Consts &c, int i, int j) { return init_liquid(c, i, j) ? c.rho1 : c.rho0; }
+
+/* FROMRIGHT's phi strip starts one column left of its T strip */
+BGK_HD double init_phi(const Consts &c, int i)
+{
+    return ((c.heat & BGK_HEAT_RIGHT) ? i >= c.Nx - c.interf : i <= c.interf) ? 1.0 : -1.0;
+}
+
 /* The nine equilibrium polynomials of STEP_7/collision.f90:19-27
  * (and initialization.f90:110-118, BC_g.f90:13-15,25-27): the factor that
  * multiplies w_k*rho (or w_k*T).  Note 4.5d0*upv*upv == (4.5*upv)*upv. */

@@ -321,6 +321,8 @@ int bgk_internal_prepare_fused(bgk_ctx *c)
 {
     if (!all_bc4(c->p))
         return fail(BGK_ERR_UNSUPPORTED, "the fused step implements the no-slip code 4 on every wall");
+    if (c->opt.heat & BGK_HEAT_RIGHT)
+        return fail(BGK_ERR_UNSUPPORTED, "BGK_HEAT_RIGHT runs on bgk_step and the stage entry points only");
     int rc = set_device(c);
     if (rc) return rc;
     if ((rc = ensure_fused(c))) return rc;
@@ -381,8 +383,11 @@ int bgk_create(const bgk_params *pp, const bgk_options *opt, bgk_ctx **out)
     *out = nullptr;
     int rc = check_params(*pp);
     if (rc) return rc;
-    bgk_options o{BGK_PREC_F64, BGK_TANH_PORTABLE, 0, -1, 0};
+    bgk_options o{BGK_PREC_F64, BGK_TANH_PORTABLE, 0, -1, 0, BGK_HEAT_WEST};
     if (opt) o = *opt;
+    if (o.heat < 0 || o.heat > (BGK_HEAT_RIGHT | BGK_HEAT_BOTTOM)) return fail(BGK_ERR_ARG, "bad heat bits %d", o.heat);
+    if ((o.heat & BGK_HEAT_RIGHT) && o.precision != BGK_PREC_F64)
+        return fail(BGK_ERR_UNSUPPORTED, "BGK_HEAT_RIGHT is implemented in the FP64 forms only");
     if (o.precision < BGK_PREC_F64 || o.precision > BGK_PREC_F32X) return fail(BGK_ERR_ARG, "bad precision %d", o.precision);
     if (o.tanh_mode != BGK_TANH_DEVICE && o.tanh_mode != BGK_TANH_PORTABLE) return fail(BGK_ERR_ARG, "bad tanh_mode");
     /* the FP32 and FP16 forms are bit-exact with nothing: CUDA's tanhf */
@@ -411,6 +416,7 @@ int bgk_create(const bgk_params *pp, const bgk_options *opt, bgk_ctx **out)
     c->p = *pp;
     c->opt = o;
     c->c = make_consts(*pp);
+    c->c.heat = o.heat;
     c->dev = dev;
     c->Nx = pp->Nx;
     c->Ny = pp->Ny;
@@ -440,6 +446,8 @@ int bgk_create(const bgk_params *pp, const bgk_options *opt, bgk_ctx **out)
     if (const char *v = getenv("BGK_PIPE")) c->tune_pipe = atoi(v);
     if (const char *v = getenv("BGK_PIPE_D")) c->tune_D = atoi(v);
     if (const char *v = getenv("BGK_PIPE_CTAS")) c->tune_ctas = atoi(v);
+    c->tune_sched = 0;
+    if (const char *v = getenv("BGK_SCHED")) c->tune_sched = atoi(v);
     c->tune_flow = 0;
     if (const char *v = getenv("BGK_FLOW")) c->tune_flow = atoi(v);
     c->flow_stall = 0;
@@ -484,13 +492,23 @@ int bgk_create(const bgk_params *pp, const bgk_options *opt, bgk_ctx **out)
     c->red_n = 4 + 4 * 592;
     DA(c->red, (size_t)c->red_n * sizeof(double), "reduction");
     DA(c->corner, 2 * sizeof(double), "corners");
-    /* walls other than the no-slip code 4 (FP64 only): the f halo ring */
-    c->ring = o.precision == BGK_PREC_F64 && !all_bc4(*pp);
+    /* walls other than the no-slip code 4 (FP64 only): the f halo ring.
+     * BGK_HEAT_RIGHT runs there too: its west g halos take T(1,j) of the
+     * previous step, which the ring step keeps in the T mirror (edge nodes
+     * write their moments every step) and bc_prep reads before each step */
+    c->ring = o.precision == BGK_PREC_F64 && (!all_bc4(*pp) || (o.heat & BGK_HEAT_RIGHT));
     c->ring_len = bgk::ring_length(c->Nx, c->Ny);
     c->fring = nullptr;
     if (c->ring) {
         DA(c->fring, (size_t)9 * (size_t)c->ring_len * sizeof(double), "f halo ring");
         CK(cudaMemsetAsync(c->fring, 0, (size_t)9 * (size_t)c->ring_len * sizeof(double), c->stream), "memset");
+    }
+    c->tright = nullptr;
+    if (o.heat & BGK_HEAT_RIGHT) {
+        DA(c->tright, (size_t)c->Ny * sizeof(double), "east T column");
+        std::vector<double> col((size_t)c->Ny, c->c.Tin);
+        e = cudaMemcpy(c->tright, col.data(), col.size() * sizeof(double), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) { bgk_destroy(c); return cuda_fail(e, "east T column"); }
     }
     e = cudaMallocHost(&c->pinned, 64 * sizeof(double));
     if (e != cudaSuccess) { bgk_destroy(c); return cuda_fail(e, "cudaMallocHost"); }
@@ -507,7 +525,7 @@ int bgk_destroy(bgk_ctx *c)
     void *ptrs[] = {c->raw[0], c->raw[1], c->raw[2], c->raw[3], c->raw[4], c->raw[5], c->errflag,
                     c->tcol[0], c->tcol[1], c->gW, c->pE, c->phiW, c->phiE, c->tin_rows,
                     c->mrho, c->mT, c->mu, c->mv, c->mphi, c->sphip, c->srho2, c->sT2, c->su2, c->sv2,
-                    c->scratch, c->red, c->corner, c->fring, c->flow_buf};
+                    c->scratch, c->red, c->corner, c->fring, c->flow_buf, c->tright};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (int k = 0; k < 9; k++) {
@@ -732,6 +750,8 @@ static int rows_copy(bgk_ctx *c, int j0, int nrows, const void *buf, bool unpack
     if (!all_bc4(c->p))
         return fail(BGK_ERR_UNSUPPORTED, "packed rows belong to the fused step, which implements the no-slip "
                                          "code 4 on every wall");
+    if (c->opt.heat)
+        return fail(BGK_ERR_UNSUPPORTED, "the packed-row exchange implements the heated west wall only");
     int rc = set_device(c);
     if (rc) return rc;
     cudaPointerAttributes at;
@@ -778,6 +798,8 @@ int bgk_set_tin(bgk_ctx *c, const double *tin, int ny)
         return BGK_OK;
     }
     if (ny != c->Ny) return fail(BGK_ERR_ARG, "tin has %d rows, expected Ny = %d", ny, c->Ny);
+    if (c->opt.heat & BGK_HEAT_RIGHT)
+        return fail(BGK_ERR_UNSUPPORTED, "a per-row tin sets the west wall, which BGK_HEAT_RIGHT leaves adiabatic");
     for (int j = 0; j < ny; j++)
         if (!std::isfinite(tin[j])) return fail(BGK_ERR_ARG, "tin[%d] is not finite", j);
     if (!c->tin_rows) {

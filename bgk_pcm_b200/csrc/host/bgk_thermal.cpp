@@ -11,8 +11,11 @@
  * reference's own main.f90 against the C ABI (the binding a Fortran host
  * would use is bgk_pcm_b200/fortran/bgk_c.f90).
  *
- * usage: bgk_thermal [dir] [--precision f64|f32|f16|f32x] [--fma] [--tanh portable]
+ * usage: bgk_thermal [dir] [--precision f64|f32|f16|f32x] [--fma] [--tanh portable|device]
+ *                    [--heat west|right|bottom|right+bottom]
  *                    [--snapshot-in file] [--snapshot-out file] [--dump-out]
+ * --heat selects the heated wall of the reference's STEP_DOCONCURRENT build
+ * options (right = FROMRIGHT, bottom = FROMBOTTOM, both = both macros).
  * dump != 0 in input.dat restarts from the reference's text dump
  * (dumpFile.dat, plus dumpPhi.dat when present); --dump-out writes both at
  * the end of the run.
@@ -387,7 +390,7 @@ int main(int argc, char **argv)
 {
     Ctx c;
     c.dir = ".";
-    bgk_options opt{BGK_PREC_F64, BGK_TANH_DEVICE, 0, -1, 0};
+    bgk_options opt{BGK_PREC_F64, BGK_TANH_PORTABLE, 0, -1, 0, BGK_HEAT_WEST};
     std::string snap_in, snap_out;
     bool dump_at_end = false;
     for (int a = 1; a < argc; a++) {
@@ -399,7 +402,16 @@ int main(int argc, char **argv)
         } else if (s == "--fma") {
             opt.fma = 1;
         } else if (s == "--tanh" && a + 1 < argc) {
-            opt.tanh_mode = std::string(argv[++a]) == "portable" ? BGK_TANH_PORTABLE : BGK_TANH_DEVICE;
+            opt.tanh_mode = std::string(argv[++a]) == "device" ? BGK_TANH_DEVICE : BGK_TANH_PORTABLE;
+        } else if (s == "--heat" && a + 1 < argc) {
+            const std::string v = argv[++a];
+            opt.heat = (v.find("right") != std::string::npos ? BGK_HEAT_RIGHT : 0) |
+                       (v.find("bottom") != std::string::npos ? BGK_HEAT_BOTTOM : 0);
+            if (opt.heat == 0 && v != "west") {
+                fprintf(stderr, "bgk_thermal: --heat takes west, right, bottom or right+bottom\n");
+                return 1;
+            }
+            printf(" Heating from %s\n", (opt.heat & BGK_HEAT_RIGHT) ? "right (Est wall)" : "left (West wall)");
         } else if (s == "--snapshot-in" && a + 1 < argc) {
             snap_in = argv[++a];
         } else if (s == "--snapshot-out" && a + 1 < argc) {

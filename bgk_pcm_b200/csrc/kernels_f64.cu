@@ -40,7 +40,9 @@ struct Staged {
 /* STEP_7/initialization.f90:15-152, one thread per reference cell
  * (i,j) in 0..Nx+1 x 0..Ny+1.  Writes the mirrors (rho,T,u,v,phi with halos),
  * the compact populations (interior) or the staged arrays, and phi twice
- * (phi and phi_prec are equal after initialization). */
+ * (phi and phi_prec are equal after initialization).  The heat bits select
+ * STEP_DOCONCURRENT/initialization.f90's FROMRIGHT / FROMBOTTOM branches
+ * (:16-62 T/rho, :122-137 T buffer, :208-222 phi). */
 __global__ void init_kernel(Consts c, int westBC, StepPtrs<double> s, double *fcomp, double *gcomp,
                             double *phc0, double *phc1, Staged st, bool staged, double *corner, double *tcol,
                             double *ring, long long RL)
@@ -50,10 +52,10 @@ __global__ void init_kernel(Consts c, int westBC, StepPtrs<double> s, double *fc
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= NX2 || j >= NY2) return;
     const int Nx = c.Nx, Ny = c.Ny;
-    double T = (i <= c.interf) ? c.T0 : c.T_in_sol;
-    double rho = (i <= c.interf) ? c.rho1 : c.rho0;
+    const double T = init_T(c, i, j);
+    double rho = init_rho(c, i, j);
     double u = c.u0, v = c.v0;
-    if (i == 0) T = c.Tin;
+    const size_t q = (size_t)i + (size_t)NX2 * (size_t)j;
     if (j == 0 || j == Ny + 1) { u = 0.0; v = 0.0; }
     if (westBC == 3) {
         u = 0.0; v = 0.0;
@@ -70,8 +72,7 @@ __global__ void init_kernel(Consts c, int westBC, StepPtrs<double> s, double *fc
     }
     double P[9];
     eq_poly(u, v, P);
-    double phi = (i <= c.interf) ? 1.0 : -1.0;
-    const size_t q = (size_t)i + (size_t)NX2 * (size_t)j;
+    const double phi = init_phi(c, i);
     s.mrho[q] = rho; s.mT[q] = T; s.mu[q] = u; s.mv[q] = v; s.mphi[q] = phi;
     double fe[9], ge[9];
     for (int k = 0; k < 9; k++) { fe[k] = c.w[k] * rho * P[k]; ge[k] = c.w[k] * T * P[k]; }
@@ -99,20 +100,32 @@ __global__ void init_kernel(Consts c, int westBC, StepPtrs<double> s, double *fc
 
 /* West g values (BC_g.f90:7-17) per row, the east equilibrium polynomials
  * (BC_g.f90:21-31: g_k(Nx+1,j) = w_k*T(Nx,j)*poly_k(u(Nx+1,j),v(Nx+1,j))),
- * and the frozen phi columns.  tin = per-row hot wall or null (scalar). */
+ * and the frozen phi columns.  tin = per-row hot wall or null (scalar).
+ * With BGK_HEAT_RIGHT (STEP_DOCONCURRENT/BC_g.f90:13-17) the west values are
+ * w_k*T(1,j)*poly of directions 3, 7, 6, T(1,j) being the previous step's
+ * (the T mirror, which the ring step writes at edge nodes every step); this
+ * then runs before every step. */
 __global__ void bc_prep_kernel(Consts c, const double *mu, const double *mv, const double *mphi,
-                               const double *tin, double *gW, double *pE, double *phiW, double *phiE)
+                               const double *mT, const double *tin, double *gW, double *pE, double *phiW,
+                               double *phiE)
 {
     const int Ny = c.Ny, NX2 = c.Nx + 2;
     const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
     if (j > Ny) return;
     double P[9];
     const size_t qw = (size_t)NX2 * j, qe = (size_t)(c.Nx + 1) + (size_t)NX2 * j;
-    const double Tin = tin ? tin[j - 1] : c.Tin;
     eq_poly(mu[qw], mv[qw], P);
-    gW[0 * Ny + j - 1] = c.w[1] * Tin * P[1];
-    gW[1 * Ny + j - 1] = c.w[5] * Tin * P[5];
-    gW[2 * Ny + j - 1] = c.w[8] * Tin * P[8];
+    if (c.heat & BGK_HEAT_RIGHT) {
+        const double T1 = mT[qw + 1];
+        gW[0 * Ny + j - 1] = c.w[1] * T1 * P[3];
+        gW[1 * Ny + j - 1] = c.w[5] * T1 * P[7];
+        gW[2 * Ny + j - 1] = c.w[8] * T1 * P[6];
+    } else {
+        const double Tin = tin ? tin[j - 1] : c.Tin;
+        gW[0 * Ny + j - 1] = c.w[1] * Tin * P[1];
+        gW[1 * Ny + j - 1] = c.w[5] * Tin * P[5];
+        gW[2 * Ny + j - 1] = c.w[8] * Tin * P[8];
+    }
     eq_poly(mu[qe], mv[qe], P);
     pE[0 * Ny + j - 1] = P[3];
     pE[1 * Ny + j - 1] = P[6];
@@ -319,7 +332,25 @@ __global__ void staged_bc_g(Staged s, Consts c)
     const int Nx = c.Nx, Ny = c.Ny, NX2 = Nx + 2;
     const double *w = c.w;
     double P[9];
-    for (int j = 1 + threadIdx.x; j <= Ny; j += blockDim.x) {
+    if (c.heat & BGK_HEAT_RIGHT) {
+        /* STEP_DOCONCURRENT/BC_g.f90:13-17, 35-39 (FROMRIGHT) */
+        for (int j = 1 + threadIdx.x; j <= Ny; j += blockDim.x) {
+            eq_poly(s.u[SQ(0, j)], s.v[SQ(0, j)], P);
+            const double t = s.T[SQ(1, j)];
+            s.g[1][SQ(0, j)] = w[1] * t * P[3];
+            s.g[5][SQ(0, j)] = w[5] * t * P[7];
+            s.g[8][SQ(0, j)] = w[8] * t * P[6];
+            s.T[SQ(0, j)] = s.T[SQ(1, j)];
+        }
+        for (int j = 1 + threadIdx.x; j <= Ny; j += blockDim.x) {
+            eq_poly(s.u[SQ(Nx + 1, j)], s.v[SQ(Nx + 1, j)], P);
+            s.g[3][SQ(Nx + 1, j)] = w[3] * c.Tin * P[3];
+            s.g[6][SQ(Nx + 1, j)] = w[6] * c.Tin * P[6];
+            s.g[7][SQ(Nx + 1, j)] = w[7] * c.Tin * P[7];
+            s.T[SQ(Nx + 1, j)] = c.Tin;
+        }
+    }
+    for (int j = 1 + threadIdx.x; j <= Ny && !(c.heat & BGK_HEAT_RIGHT); j += blockDim.x) {
         const double Tin = s.tin ? s.tin[j - 1] : c.Tin;
         eq_poly(s.u[SQ(0, j)], s.v[SQ(0, j)], P);
         s.g[1][SQ(0, j)] = w[1] * Tin * P[1];
@@ -327,7 +358,7 @@ __global__ void staged_bc_g(Staged s, Consts c)
         s.g[8][SQ(0, j)] = w[8] * Tin * P[8];
         s.T[SQ(0, j)] = Tin;
     }
-    for (int j = 1 + threadIdx.x; j <= Ny; j += blockDim.x) {
+    for (int j = 1 + threadIdx.x; j <= Ny && !(c.heat & BGK_HEAT_RIGHT); j += blockDim.x) {
         eq_poly(s.u[SQ(Nx + 1, j)], s.v[SQ(Nx + 1, j)], P);
         const double t = s.T[SQ(Nx, j)];
         s.g[3][SQ(Nx + 1, j)] = w[3] * t * P[3];
@@ -505,10 +536,16 @@ __global__ void ring_bc_kernel(Consts c, RingF F, double *rho, double *u, double
     }
     __syncthreads();
     /* BC_g, macroscopic part: T west/east (T(Nx,j) of the previous moments
-     * is tcol), then T and phi north/south */
+     * is tcol; with BGK_HEAT_RIGHT, T(1,j) of the previous step is in the
+     * mirror and the east wall is Tin), then T and phi north/south */
     for (int j = 1 + t0; j <= Ny; j += nt) {
-        T[SQ(0, j)] = tin ? tin[j - 1] : c.Tin;
-        T[SQ(Nx + 1, j)] = tcol[j - 1];
+        if (c.heat & BGK_HEAT_RIGHT) {
+            T[SQ(0, j)] = T[SQ(1, j)];
+            T[SQ(Nx + 1, j)] = c.Tin;
+        } else {
+            T[SQ(0, j)] = tin ? tin[j - 1] : c.Tin;
+            T[SQ(Nx + 1, j)] = tcol[j - 1];
+        }
     }
     __syncthreads();
     for (int i = t0; i <= Nx + 1; i += nt) {
@@ -798,7 +835,7 @@ cudaError_t launch_ring_bc(bgk_ctx *c)
 cudaError_t launch_bc_prep(bgk_ctx *c)
 {
     int n = c->Ny;
-    bc_prep_kernel<<<(n + 127) / 128, 128, 0, c->stream>>>(c->c, c->mu, c->mv, c->mphi, c->tin_rows,
+    bc_prep_kernel<<<(n + 127) / 128, 128, 0, c->stream>>>(c->c, c->mu, c->mv, c->mphi, c->mT, c->tin_rows,
                                                             c->gW, c->pE, c->phiW, c->phiE);
     return cudaGetLastError();
 }
@@ -833,11 +870,11 @@ static void flow_ptrs(const bgk_ctx *c, StepPtrs<double> &s0, StepPtrs<double> &
     s0.fin = (const double *)c->fbuf[a]; s0.gin = (const double *)c->gbuf[a];
     s0.fout = (double *)c->fbuf[b]; s0.gout = (double *)c->gbuf[b];
     s0.phin = (const double *)c->phibuf[a]; s0.phout = (double *)c->phibuf[b];
-    s0.tcin = c->tcol[a]; s0.tcout = c->tcol[b];
+    s0.tcin = east_tcol(c, a); s0.tcout = c->tcol[b];
     s1.fin = (const double *)c->fbuf[b]; s1.gin = (const double *)c->gbuf[b];
     s1.fout = (double *)c->fbuf[a]; s1.gout = (double *)c->gbuf[a];
     s1.phin = (const double *)c->phibuf[b]; s1.phout = (double *)c->phibuf[a];
-    s1.tcin = c->tcol[b]; s1.tcout = c->tcol[a];
+    s1.tcin = east_tcol(c, b); s1.tcout = c->tcol[a];
 }
 
 /* nsteps exact-order FP64 steps in one dataflow launch (walls of code 4). */
@@ -855,7 +892,7 @@ cudaError_t launch_fused_f64(bgk_ctx *c, bool moments)
     s.fin = (const double *)c->fbuf[src]; s.gin = (const double *)c->gbuf[src];
     s.fout = (double *)c->fbuf[dst]; s.gout = (double *)c->gbuf[dst];
     s.phin = (const double *)c->phibuf[src]; s.phout = (double *)c->phibuf[dst];
-    s.tcin = c->tcol[src]; s.tcout = c->tcol[dst];
+    s.tcin = east_tcol(c, src); s.tcout = c->tcol[dst];
     s.gW = c->gW; s.pE = c->pE; s.phiW = c->phiW; s.phiE = c->phiE;
     s.mrho = c->mrho; s.mT = c->mT; s.mu = c->mu; s.mv = c->mv; s.mphi = c->mphi;
     s.plane = c->plane; s.P = c->P; s.NX2 = c->NX2;

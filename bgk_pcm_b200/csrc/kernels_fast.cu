@@ -51,11 +51,11 @@ static void flow_ptrs(const bgk_ctx *c, StepPtrs<double> &s0, StepPtrs<double> &
     s0.fin = (const double *)c->fbuf[a]; s0.gin = (const double *)c->gbuf[a];
     s0.fout = (double *)c->fbuf[b]; s0.gout = (double *)c->gbuf[b];
     s0.phin = (const double *)c->phibuf[a]; s0.phout = (double *)c->phibuf[b];
-    s0.tcin = c->tcol[a]; s0.tcout = c->tcol[b];
+    s0.tcin = east_tcol(c, a); s0.tcout = c->tcol[b];
     s1.fin = (const double *)c->fbuf[b]; s1.gin = (const double *)c->gbuf[b];
     s1.fout = (double *)c->fbuf[a]; s1.gout = (double *)c->gbuf[a];
     s1.phin = (const double *)c->phibuf[b]; s1.phout = (double *)c->phibuf[a];
-    s1.tcin = c->tcol[b]; s1.tcout = c->tcol[a];
+    s1.tcin = east_tcol(c, b); s1.tcout = c->tcol[a];
 }
 
 cudaError_t launch_flow_lowp(bgk_ctx *c, int nsteps);
@@ -78,7 +78,7 @@ cudaError_t launch_fused_fast(bgk_ctx *c, bool moments)
     s.fin = (const double *)c->fbuf[src]; s.gin = (const double *)c->gbuf[src];
     s.fout = (double *)c->fbuf[dst]; s.gout = (double *)c->gbuf[dst];
     s.phin = (const double *)c->phibuf[src]; s.phout = (double *)c->phibuf[dst];
-    s.tcin = c->tcol[src]; s.tcout = c->tcol[dst];
+    s.tcin = east_tcol(c, src); s.tcout = c->tcol[dst];
     s.gW = c->gW; s.pE = c->pE; s.phiW = c->phiW; s.phiE = c->phiE;
     s.mrho = c->mrho; s.mT = c->mT; s.mu = c->mu; s.mv = c->mv; s.mphi = c->mphi;
     s.plane = c->plane; s.P = c->P; s.NX2 = c->NX2;
@@ -814,7 +814,7 @@ cudaError_t pipe_lp_launch(bgk_ctx *c, const LpPtrs<S, PT> &s, const ConstsLP<AT
     const cudaError_t e = pipe_configure(fused_pipe_lp_kernel<S, PT, AT, D, T, M>, smem, c->dev, done);
     if (e != cudaSuccess) return e;
     int grid;
-    const PipeSched sch = pipe_sched(c, ctas, 8, &grid);
+    const PipeSched sch = pipe_sched_step(c, ctas, 8, &grid);
     /* plain launch: programmatic dependent launch measured 3-10 % slower for
      * these forms (the kernel's griddepcontrol instructions are no-ops then) */
     fused_pipe_lp_kernel<S, PT, AT, D, T, M><<<grid, PIPE_THREADS, smem, c->stream>>>(s, lp, sch, c->errflag);
@@ -840,9 +840,9 @@ __global__ void init_lowp_kernel(Consts c, S *fd, S *gd, PT *ph0, PT *ph1, long 
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= c.Nx || y >= c.Ny) return;
-    const int i = x + 1;
-    const double T = (i <= c.interf) ? c.T0 : c.T_in_sol;
-    const double rho = (i <= c.interf) ? c.rho1 : c.rho0;
+    const int i = x + 1, j = y + 1;
+    const double T = init_T(c, i, j);
+    const double rho = init_rho(c, i, j);
     double Pq[9];
     eq_poly(c.u0, c.v0, Pq);
     const long long cc = (long long)y * P + x;
@@ -850,7 +850,7 @@ __global__ void init_lowp_kernel(Consts c, S *fd, S *gd, PT *ph0, PT *ph1, long 
         Codec<S>::st(fd + k * plane + cc, (float)(c.w[k] * rho * Pq[k] - c.w[k] * c.rho0), sf);
         Codec<S>::st(gd + k * plane + cc, (float)(c.w[k] * T * Pq[k] - c.w[k] * c.T0), sg);
     }
-    const PT phi = PhiCodec<PT>::from_d((i <= c.interf) ? 1.0 : -1.0);
+    const PT phi = PhiCodec<PT>::from_d(init_phi(c, i));
     ph0[cc] = phi;
     ph1[cc] = phi;
 }

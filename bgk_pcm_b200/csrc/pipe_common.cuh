@@ -22,6 +22,12 @@ constexpr long long PIPE_WAIT_LIMIT = 1LL << 24;   /* x ~64 ns sleeps: ~1 s */
 struct PipeSched {
     int nbands, H, nstrips, ntiles;
     int bx;                 /* band (tile) width in columns */
+    int ranges;             /* 0: tiles t = blockIdx.x, +gridDim.x, ... of H
+                             * rows; 1: CTA b takes rows [b*L/G, (b+1)*L/G)
+                             * of the band-major row sequence (band 0 rows
+                             * 0..Ny-1, then band 1, ...; L = nbands*Ny, G =
+                             * gridDim.x), i.e. equal work to within a row
+                             * and no partial last wave */
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -86,15 +92,24 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
 }
 
 /* Iterate this CTA's work items in order: tiles t = blockIdx.x, +gridDim.x,
- * ..., rows y0..y1-1 of each.  next() returns false at the end. */
+ * ..., rows y0..y1-1 of each; or, with sch.ranges, the CTA's range of the
+ * band-major row sequence, one tile per band it touches (t = the band).
+ * next() returns false at the end. */
 struct PipeIter {
     int t, y, y1, x0;
+    long long r, rend;     /* ranges: next row of the sequence, end of ours */
     PipeSched sch;
     int Ny;
     __device__ bool start(const PipeSched &s, int Ny_)
     {
         sch = s;
         Ny = Ny_;
+        if (sch.ranges) {
+            const long long L = (long long)sch.nbands * Ny;
+            r = L * blockIdx.x / gridDim.x;
+            rend = L * (blockIdx.x + 1) / gridDim.x;
+            return open_range();
+        }
         t = blockIdx.x;
         return open();
     }
@@ -107,8 +122,23 @@ struct PipeIter {
         y1 = min(y + sch.H, Ny);
         return true;
     }
+    __device__ bool open_range()
+    {
+        if (r >= rend) return false;
+        t = (int)(r / Ny);
+        x0 = t * sch.bx;
+        y = (int)(r - (long long)t * Ny);
+        const long long left = rend - r;
+        y1 = left < (long long)(Ny - y) ? y + (int)left : Ny;
+        return true;
+    }
     __device__ bool next()
     {
+        if (sch.ranges) {
+            ++r;
+            if (++y < y1) return true;
+            return open_range();
+        }
         if (++y < y1) return true;
         t += gridDim.x;
         return open();
@@ -121,7 +151,7 @@ struct PipeIter {
  * 4 tiles per resident CTA (small grids, e.g. 512^2 runs best at H = 1). */
 inline PipeSched pipe_sched(const bgk_ctx *c, int ctas_per_sm, int base_H, int *grid)
 {
-    PipeSched sch;
+    PipeSched sch{};
     sch.bx = PIPE_BX;
     sch.nbands = (c->Nx + PIPE_BX - 1) / PIPE_BX;
     const long long slots = (long long)c->nsm * ctas_per_sm;
@@ -131,7 +161,22 @@ inline PipeSched pipe_sched(const bgk_ctx *c, int ctas_per_sm, int base_H, int *
     sch.H = H;
     sch.nstrips = (c->Ny + H - 1) / H;
     sch.ntiles = sch.nbands * sch.nstrips;
+    sch.ranges = 0;
     *grid = (int)(sch.ntiles < slots ? sch.ntiles : slots);
+    return sch;
+}
+
+/* The per-step pipeline's schedule: tiles (pipe_sched), or with
+ * BGK_SCHED=1 equal row ranges, one per resident CTA slot. */
+inline PipeSched pipe_sched_step(const bgk_ctx *c, int ctas_per_sm, int base_H, int *grid)
+{
+    PipeSched sch = pipe_sched(c, ctas_per_sm, base_H, grid);
+    if (c->tune_sched == 1) {
+        const long long L = (long long)sch.nbands * c->Ny;
+        const long long slots = (long long)c->nsm * ctas_per_sm;
+        sch.ranges = 1;
+        *grid = (int)(L < slots ? L : slots);
+    }
     return sch;
 }
 

@@ -12,6 +12,7 @@ module bgk_c
                                BGK_ERR_OOM = -4, BGK_ERR_STATE = -5, BGK_ERR_IO = -6, BGK_ERR_NONFINITE = -7
   integer(c_int), parameter :: BGK_PREC_F64 = 0, BGK_PREC_F32 = 1, BGK_PREC_F16 = 2, BGK_PREC_F32X = 3
   integer(c_int), parameter :: BGK_TANH_PORTABLE = 0, BGK_TANH_DEVICE = 1
+  integer(c_int), parameter :: BGK_HEAT_WEST = 0, BGK_HEAT_RIGHT = 1, BGK_HEAT_BOTTOM = 2
   integer(c_int), parameter :: BGK_FIELD_F0 = 0, BGK_FIELD_G0 = 9
   integer(c_int), parameter :: BGK_FIELD_RHO = 18, BGK_FIELD_T = 19, BGK_FIELD_U = 20, BGK_FIELD_V = 21
   integer(c_int), parameter :: BGK_FIELD_PHI = 22, BGK_FIELD_PHI_PREC = 23
@@ -32,7 +33,7 @@ module bgk_c
   end type bgk_adjoint_spec
 
   type, bind(c) :: bgk_options
-     integer(c_int) :: precision, tanh_mode, fma, device, smooth
+     integer(c_int) :: precision, tanh_mode, fma, device, smooth, heat
   end type bgk_options
 
   interface

@@ -23,6 +23,19 @@ _PREC = {"f64": capi.PREC_F64, "f32": capi.PREC_F32, "f16": capi.PREC_F16, "f32x
 _TANH = {"device": capi.TANH_DEVICE, "portable": capi.TANH_PORTABLE}
 
 
+def heat_bits(heat) -> int:
+    """The heated wall: "west" (STEP_7), "right" (STEP_DOCONCURRENT's
+    FROMRIGHT), "bottom" (FROMBOTTOM), "right+bottom" (both macros), or the
+    BGK_HEAT_* bits as an int."""
+    if isinstance(heat, int):
+        return heat
+    bits = {"west": capi.HEAT_WEST, "right": capi.HEAT_RIGHT, "bottom": capi.HEAT_BOTTOM}
+    try:
+        return sum(bits[h] for h in str(heat).split("+"))
+    except KeyError:
+        raise ValueError(f"heat must be west, right, bottom or right+bottom, not {heat!r}") from None
+
+
 def _dptr(a: np.ndarray):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
@@ -31,14 +44,15 @@ class Solver:
     """One simulation on one B200 (STEP_7/setup.f90 allocates, this creates)."""
 
     def __init__(self, params, precision: str = "f64", tanh: str = "portable", fma: bool = False,
-                 device: int = -1, smooth: bool = False):
+                 device: int = -1, smooth: bool = False, heat="west"):
         lib = capi.load()
         if isinstance(params, dict):
             params = capi.Params.from_dict(params)
         self.params = params
         self.Nx, self.Ny = params.Nx, params.Ny
         self.precision = precision
-        opt = capi.Options(_PREC[precision], _TANH[tanh], 1 if fma else 0, device, 1 if smooth else 0)
+        self.heat = heat_bits(heat)
+        opt = capi.Options(_PREC[precision], _TANH[tanh], 1 if fma else 0, device, 1 if smooth else 0, self.heat)
         h = ctypes.c_void_p()
         capi.check(lib.bgk_create(ctypes.byref(params), ctypes.byref(opt), ctypes.byref(h)))
         self._h = h

@@ -78,7 +78,31 @@ typedef struct bgk_options {
                      /* STEP_7/collision.f90:84-120 (implicitly typed); 1 = keep */
                      /* them in double, which makes the step a smooth function   */
                      /* of its inputs (the form the adjoint differentiates)      */
+    int heat;        /* BGK_HEAT_* bits: the heated wall (0 = west, STEP_7)      */
 } bgk_options;
+
+/* Heating options of the reference's STEP_DOCONCURRENT variant, which it
+ * selects with preprocessor macros at build time; here they are bits of
+ * bgk_options.heat, chosen at bgk_create:
+ *  BGK_HEAT_RIGHT  (FROMRIGHT, STEP_DOCONCURRENT/BC_g.f90:13-45 and
+ *                  initialization.f90:30-60,128-133,208-214): the east wall
+ *                  is held at Tin and the west wall is zero-gradient in T
+ *                  (its g1, g5, g8 use the polynomials of directions 3, 7, 6,
+ *                  with T(1,j) of the previous step); the initial liquid
+ *                  strip is T/rho at columns >= Nx-interf+1 and phi at
+ *                  columns >= Nx-interf.  FP64 forms only.
+ *  BGK_HEAT_BOTTOM (FROMBOTTOM, initialization.f90:16-28,123-127): the
+ *                  initial liquid layer is rows 0..interf (interf = Nx/40);
+ *                  the walls are STEP_7's.  Its T buffer loop `T(i,0) = Tin,
+ *                  i = 0..Ny+1` runs along x and, with Ny > Nx, on into row
+ *                  1; that is reproduced.  Every precision form.
+ * Both bits = both macros defined (T/rho layer from FROMBOTTOM, phi strip and
+ * walls from FROMRIGHT).  The packed-row exchange (the y-slab
+ * decomposition) refuses both bits; bgk_advance and the adjoint refuse
+ * BGK_HEAT_RIGHT. */
+#define BGK_HEAT_WEST    0
+#define BGK_HEAT_RIGHT   1
+#define BGK_HEAT_BOTTOM  2
 
 /* ----------------------------------------------------------------- fields */
 /* Field ids for bgk_upload / bgk_download; the names are the reference's
@@ -110,8 +134,8 @@ int bgk_read_input(const char *path, bgk_params *out);
 
 /* Allocate device state and derive the constants (weights, omega_f, omega_g,
  * kvisc, alpha).  Replaces STEP_7/setup.f90:34-115.  opt may be NULL
- * (FP64, portable tanh, exact order, current device: the same as a
- * zero-initialized bgk_options).  Walls: the FP64 step (fused and staged)
+ * (FP64, portable tanh, exact order, current device, heated west wall: the
+ * same as a zero-initialized bgk_options).  Walls: the FP64 step (fused and staged)
  * runs every BC_f code of STEP_7/BC_f.f90 (0 periodic, 1 fixed velocity, 2
  * parabolic inflow, 3 fixed pressure, 4 no-slip, 5 symmetric, 6 open); with
  * a wall other than code 4 the fused step keeps the f halo cells in a ring
@@ -177,7 +201,8 @@ int bgk_set_it(bgk_ctx *ctx, int it);
 
 /* Hot-wall temperature per row: tin[j-1] is Tin for row j = 1..Ny
  * (generalises the scalar Tin of STEP_7/BC_g.f90:13-16; tin = NULL restores
- * the scalar Tin = T0 of STEP_7/initialization.f90:9). */
+ * the scalar Tin = T0 of STEP_7/initialization.f90:9).  The heated wall is
+ * the west one: a context created with BGK_HEAT_RIGHT refuses a per-row tin. */
 int bgk_set_tin(bgk_ctx *ctx, const double *tin, int ny);
 
 /* Wait for all work queued on the context's stream. */
