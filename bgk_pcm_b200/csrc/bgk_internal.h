@@ -161,8 +161,6 @@ struct bgk_ctx {
      * pulls; pipeline depth and CTAs per SM (BGK_PIPE, BGK_PIPE_D,
      * BGK_PIPE_CTAS) */
     int tune_pipe, tune_D, tune_ctas, nsm;
-    int tune_sched;        /* per-step pipeline schedule: 0 tiles, 1 equal row
-                            * ranges (BGK_SCHED)                            */
     int tune_flow;         /* 1: reduced-precision steps between outputs in one
                             * dataflow launch (BGK_FLOW)                    */
     void *flow_buf;        /* its ticket counter and per-tile step counts   */

@@ -446,8 +446,6 @@ int bgk_create(const bgk_params *pp, const bgk_options *opt, bgk_ctx **out)
     if (const char *v = getenv("BGK_PIPE")) c->tune_pipe = atoi(v);
     if (const char *v = getenv("BGK_PIPE_D")) c->tune_D = atoi(v);
     if (const char *v = getenv("BGK_PIPE_CTAS")) c->tune_ctas = atoi(v);
-    c->tune_sched = 0;
-    if (const char *v = getenv("BGK_SCHED")) c->tune_sched = atoi(v);
     c->tune_flow = 0;
     if (const char *v = getenv("BGK_FLOW")) c->tune_flow = atoi(v);
     c->flow_stall = 0;

@@ -814,7 +814,7 @@ cudaError_t pipe_lp_launch(bgk_ctx *c, const LpPtrs<S, PT> &s, const ConstsLP<AT
     const cudaError_t e = pipe_configure(fused_pipe_lp_kernel<S, PT, AT, D, T, M>, smem, c->dev, done);
     if (e != cudaSuccess) return e;
     int grid;
-    const PipeSched sch = pipe_sched_step(c, ctas, 8, &grid);
+    const PipeSched sch = pipe_sched(c, ctas, 8, &grid);
     /* plain launch: programmatic dependent launch measured 3-10 % slower for
      * these forms (the kernel's griddepcontrol instructions are no-ops then) */
     fused_pipe_lp_kernel<S, PT, AT, D, T, M><<<grid, PIPE_THREADS, smem, c->stream>>>(s, lp, sch, c->errflag);
