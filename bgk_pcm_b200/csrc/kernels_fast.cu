@@ -813,6 +813,10 @@ cudaError_t pipe_lp_launch(bgk_ctx *c, const LpPtrs<S, PT> &s, const ConstsLP<AT
     static std::atomic<unsigned long long> done{0};
     const cudaError_t e = pipe_configure(fused_pipe_lp_kernel<S, PT, AT, D, T, M>, smem, c->dev, done);
     if (e != cudaSuccess) return e;
+    /* no more CTAs per SM in the grid than can be resident */
+    static std::atomic<int> occ{0};
+    const int fit = pipe_occupancy(fused_pipe_lp_kernel<S, PT, AT, D, T, M>, smem, occ);
+    if (fit > 0 && ctas > fit) ctas = fit;
     int grid;
     const PipeSched sch = pipe_sched(c, ctas, 8, &grid);
     /* plain launch: programmatic dependent launch measured 3-10 % slower for
@@ -968,12 +972,13 @@ cudaError_t launch_lowp_t(bgk_ctx *c, bool moments)
     const int H = strip_height(c);
     dim3 grd((c->Nx + FUSED_BX - 1) / FUSED_BX, (c->Ny + H - 1) / H);
     if (c->tune_pipe) {
-        /* stages of ~10 KB (FP32) / ~5 KB (FP16).  Measured on B200 at 2048^2
-         * and 4096^2 (sweep of 3..6 stages x 3..5 CTAs per SM): 4 stages
-         * with 4 CTAs per SM is best for both forms at 4096^2 and within 3 %
-         * of the best at 2048^2. */
+        /* stages of ~10 KB (FP32) / ~5 KB (FP16).  Measured on B200 (FP32,
+         * 3/4 stages x 4/5 CTAs per SM x H = 4/8/16 at 1024^2, 2048^2,
+         * 3072^2, 4096^2 and 16384x4096): 4 stages; 5 CTAs per SM up to
+         * 2^22 nodes (+7 % at 1024^2, +13 % at 2048^2: 35.4 against 31.3
+         * GLUPS), 4 above (5 loses 3-16 % there). */
         const int D = c->tune_D > 0 ? c->tune_D : 4;
-        const int ctas = c->tune_ctas > 0 ? c->tune_ctas : 4;
+        const int ctas = c->tune_ctas > 0 ? c->tune_ctas : ((long long)c->Nx * c->Ny <= (1LL << 22) ? 5 : 4);
         if (D <= 3) return pipe_lp_dispatch<S, PT, AT, 3>(c, s, lp, moments, ctas);
         if (D >= 6) return pipe_lp_dispatch<S, PT, AT, 6>(c, s, lp, moments, ctas);
         return pipe_lp_dispatch<S, PT, AT, 4>(c, s, lp, moments, ctas);

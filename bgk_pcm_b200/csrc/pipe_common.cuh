@@ -118,18 +118,24 @@ struct PipeIter {
     }
 };
 
-/* Tile height: base_H rows (measured best on B200: 4 for FP64, 8 for the
- * reduced-precision forms; taller tiles leave a partial last wave, shorter
- * ones lose a little per tile), halved down to 1 while there are fewer than
- * 4 tiles per resident CTA (small grids, e.g. 512^2 runs best at H = 1). */
-inline PipeSched pipe_sched(const bgk_ctx *c, int ctas_per_sm, int base_H, int *grid)
+/* Tile height: max_H rows, halved down to base_H while there are fewer
+ * than 10 tiles per resident CTA, then down to 1 while there are fewer than
+ * 4 (small grids, e.g. 512^2 runs best at H = 1).  Taller tiles start fewer
+ * phase-field windows and pipeline fills; shorter ones leave a smaller
+ * partial last wave.  Measured on B200 (FP64, 200 steps): max_H = 32 gives
+ * H = 4 at 2048^2 (18.9 GLUPS; 8/16/32: 18.6/17.8/16.5), 16 at 3072^2 and
+ * 4096^2 (+1.5 %, +2.7 % over H = 4) and 32 at 16384x4096 (+2.6 %); the
+ * reduced-precision forms run best at H = 8 throughout (max_H = base_H). */
+inline PipeSched pipe_sched(const bgk_ctx *c, int ctas_per_sm, int base_H, int *grid, int max_H = 0)
 {
     PipeSched sch{};
     sch.bx = PIPE_BX;
     sch.nbands = (c->Nx + PIPE_BX - 1) / PIPE_BX;
     const long long slots = (long long)c->nsm * ctas_per_sm;
-    int H = base_H;
-    while (H > 1 && (long long)sch.nbands * ((c->Ny + H - 1) / H) < 4 * slots) H /= 2;
+    auto tiles = [&](int h) { return (long long)sch.nbands * ((c->Ny + h - 1) / h); };
+    int H = max_H > base_H ? max_H : base_H;
+    while (H > base_H && tiles(H) < 10 * slots) H /= 2;
+    while (H > 1 && tiles(H) < 4 * slots) H /= 2;
     if (c->tune_H > 0) H = c->tune_H;
     sch.H = H;
     sch.nstrips = (c->Ny + H - 1) / H;
@@ -149,6 +155,22 @@ inline cudaError_t pipe_configure(K kernel, size_t smem, int dev, std::atomic<un
     const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_release);
     return e;
+}
+
+/* Resident CTAs per SM of a pipeline kernel with `smem` bytes of dynamic
+ * shared memory (registers and shared memory decide), queried once per
+ * kernel; 0 if the query fails. */
+template <typename K>
+inline int pipe_occupancy(K kernel, size_t smem, std::atomic<int> &cached)
+{
+    int n = cached.load(std::memory_order_acquire);
+    if (n > 0) return n;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, PIPE_THREADS, smem) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return 0;
+    }
+    cached.store(n, std::memory_order_release);
+    return n;
 }
 
 /* Programmatic dependent launch.  Where it pays (the FP64 step on small
