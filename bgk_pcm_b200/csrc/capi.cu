@@ -377,6 +377,13 @@ int bgk_read_input(const char *path, bgk_params *out)
     return BGK_OK;
 }
 
+/* CK for bgk_create once the context exists: free it before failing */
+#define CKC(call, what)                                                    \
+    do {                                                                   \
+        cudaError_t e_ = (call);                                           \
+        if (e_ != cudaSuccess) { bgk_destroy(c); return cuda_fail(e_, what); } \
+    } while (0)
+
 int bgk_create(const bgk_params *pp, const bgk_options *opt, bgk_ctx **out)
 {
     if (!pp || !out) return fail(BGK_ERR_ARG, "null argument");
@@ -466,16 +473,16 @@ int bgk_create(const bgk_params *pp, const bgk_options *opt, bgk_ctx **out)
         DA(c->raw[b], popbytes + 2 * guard, "f populations");
         DA(c->raw[2 + b], popbytes + 2 * guard, "g populations");
         DA(c->raw[4 + b], phibytes + 2 * guard, "phi");
-        CK(cudaMemsetAsync(c->raw[b], 0, popbytes + 2 * guard, c->stream), "memset");
-        CK(cudaMemsetAsync(c->raw[2 + b], 0, popbytes + 2 * guard, c->stream), "memset");
-        CK(cudaMemsetAsync(c->raw[4 + b], 0, phibytes + 2 * guard, c->stream), "memset");
+        CKC(cudaMemsetAsync(c->raw[b], 0, popbytes + 2 * guard, c->stream), "memset");
+        CKC(cudaMemsetAsync(c->raw[2 + b], 0, popbytes + 2 * guard, c->stream), "memset");
+        CKC(cudaMemsetAsync(c->raw[4 + b], 0, phibytes + 2 * guard, c->stream), "memset");
         c->fbuf[b] = (char *)c->raw[b] + guard;
         c->gbuf[b] = (char *)c->raw[2 + b] + guard;
         c->phibuf[b] = (char *)c->raw[4 + b] + guard;
         DA(c->tcol[b], (size_t)c->Ny * sizeof(double), "T column");
     }
     DA(c->errflag, sizeof(int), "error flag");
-    CK(cudaMemsetAsync(c->errflag, 0, sizeof(int), c->stream), "memset");
+    CKC(cudaMemsetAsync(c->errflag, 0, sizeof(int), c->stream), "memset");
     DA(c->gW, 3 * (size_t)c->Ny * sizeof(double), "west g");
     DA(c->pE, 3 * (size_t)c->Ny * sizeof(double), "east poly");
     DA(c->phiW, (size_t)c->Ny * sizeof(double), "phi west");
@@ -499,7 +506,7 @@ int bgk_create(const bgk_params *pp, const bgk_options *opt, bgk_ctx **out)
     c->fring = nullptr;
     if (c->ring) {
         DA(c->fring, (size_t)9 * (size_t)c->ring_len * sizeof(double), "f halo ring");
-        CK(cudaMemsetAsync(c->fring, 0, (size_t)9 * (size_t)c->ring_len * sizeof(double), c->stream), "memset");
+        CKC(cudaMemsetAsync(c->fring, 0, (size_t)9 * (size_t)c->ring_len * sizeof(double), c->stream), "memset");
     }
     c->tright = nullptr;
     if (o.heat & BGK_HEAT_RIGHT) {
@@ -510,7 +517,7 @@ int bgk_create(const bgk_params *pp, const bgk_options *opt, bgk_ctx **out)
     }
     e = cudaMallocHost(&c->pinned, 64 * sizeof(double));
     if (e != cudaSuccess) { bgk_destroy(c); return cuda_fail(e, "cudaMallocHost"); }
-    CK(cudaStreamSynchronize(c->stream), "create");
+    CKC(cudaStreamSynchronize(c->stream), "create");
     *out = c;
     return BGK_OK;
 }
