@@ -853,7 +853,8 @@ int bgk_save(bgk_ctx *c, const char *path)
     if ((rc = ensure_fused(c))) return rc;
     FILE *fp = fopen(path, "wb");
     if (!fp) return fail(BGK_ERR_IO, "cannot write %s", path);
-    const int hdr[8] = {c->Nx, c->Ny, c->opt.precision, c->it, c->P, c->tin_host ? 1 : 0, c->ring ? 1 : 0, 0};
+    const int hdr[8] = {c->Nx, c->Ny, c->opt.precision, c->it, c->P, c->tin_host ? 1 : 0, c->ring ? 1 : 0,
+                        c->opt.heat};
     bool ok = fwrite(kMagic, 1, 8, fp) == 8 && fwrite(hdr, sizeof hdr, 1, fp) == 1;
     const size_t popbytes = (size_t)9 * c->plane * c->esz;
     const size_t phibytes = (size_t)c->plane * c->phisz;
@@ -899,6 +900,10 @@ int bgk_load(bgk_ctx *c, const char *path)
         fclose(fp);
         return fail(BGK_ERR_ARG, "snapshot is %dx%d precision %d; context is %dx%d precision %d", hdr[0], hdr[1],
                     hdr[2], c->Nx, c->Ny, c->opt.precision);
+    }
+    if (hdr[7] != c->opt.heat) {
+        fclose(fp);
+        return fail(BGK_ERR_ARG, "snapshot was written with heat bits %d; the context has %d", hdr[7], c->opt.heat);
     }
     const size_t popbytes = (size_t)9 * c->plane * c->esz;
     const size_t phibytes = (size_t)c->plane * c->phisz;

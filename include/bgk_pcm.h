@@ -327,8 +327,8 @@ int bgk_field_sums_rows(bgk_ctx *ctx, int j0, int nrows, double out[4]);
 
 /* Complete binary snapshot (populations, phi, frozen boundary values, it)
  * -- unlike the reference's text dump (STEP_7/dump_out.f90:5-18), which omits
- * phi and phi_prec.  A snapshot restores into a context of the same size and
- * precision. */
+ * phi and phi_prec.  A snapshot restores into a context of the same size,
+ * precision and heat bits (BGK_ERR_ARG otherwise). */
 int bgk_save(bgk_ctx *ctx, const char *path);
 int bgk_load(bgk_ctx *ctx, const char *path);
 

@@ -185,3 +185,21 @@ def test_host_program_heat_right_matches_oracle_program(tmp_path, oracle_mod, li
     for name in ["fort.666", "fort.667", "fort.668", "non-dim_bulk_numbers.dat", "Output_00002000.vtk"]:
         np.testing.assert_array_equal(numbers(dirs["gpu"] / name), numbers(dirs["oracle"] / name), err_msg=name)
     np.testing.assert_allclose(numbers(dirs["gpu"] / "fort.64"), numbers(dirs["oracle"] / "fort.64"), rtol=1e-7)
+
+
+def test_heat_snapshot_round_trip_and_mismatch(oracle_mod, lib, tmp_path):
+    """A FROMRIGHT snapshot restores bit for bit into a FROMRIGHT context
+    and is refused by a west-heated one."""
+    from bgk_pcm_b200 import Solver, capi
+    o, s = _pair(oracle_mod, 44, 12, RIGHT)
+    s.step(3); o.step(3)
+    s.save(tmp_path / "right.bin")
+    b = Solver(s.params, tanh="portable", heat="right")
+    b.load(tmp_path / "right.bin")
+    b.step(4); o.step(4)
+    _assert_equal(o, b, "after a snapshot round trip", f_halos=True)
+    w = Solver(s.params, tanh="portable")
+    with pytest.raises(capi.BGKError, match="heat"):
+        w.load(tmp_path / "right.bin")
+    for x in (w, b, s, o):
+        x.close()
