@@ -895,15 +895,15 @@ int bgk_load(bgk_ctx *c, const char *path)
     int hdr[8];
     bool ok = fread(mg, 1, 8, fp) == 8 && memcmp(mg, kMagic, 8) == 0 && fread(hdr, sizeof hdr, 1, fp) == 1;
     if (!ok) { fclose(fp); return fail(BGK_ERR_IO, "%s is not a snapshot", path); }
+    if (hdr[7] != c->opt.heat) {
+        fclose(fp);
+        return fail(BGK_ERR_ARG, "snapshot was written with heat bits %d; the context has %d", hdr[7], c->opt.heat);
+    }
     if (hdr[0] != c->Nx || hdr[1] != c->Ny || hdr[2] != c->opt.precision || hdr[4] != c->P ||
         hdr[6] != (c->ring ? 1 : 0)) {
         fclose(fp);
         return fail(BGK_ERR_ARG, "snapshot is %dx%d precision %d; context is %dx%d precision %d", hdr[0], hdr[1],
                     hdr[2], c->Nx, c->Ny, c->opt.precision);
-    }
-    if (hdr[7] != c->opt.heat) {
-        fclose(fp);
-        return fail(BGK_ERR_ARG, "snapshot was written with heat bits %d; the context has %d", hdr[7], c->opt.heat);
     }
     const size_t popbytes = (size_t)9 * c->plane * c->esz;
     const size_t phibytes = (size_t)c->plane * c->phisz;
