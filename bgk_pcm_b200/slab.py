@@ -241,6 +241,10 @@ class SlabRun:
             # slab: an inflow or pressure code would be built from the slab's
             # own rows (STEP_7/BC_f.f90:7-60) and be wrong on every slab
             raise ValueError(f"SlabRun needs the no-slip code 4 on every wall, got W/E/N/S = {walls}")
+        if solver_kw.get("heat", "west") not in ("west", 0):
+            # the heating options place the initial liquid layer and the hot
+            # wall by global rows and columns; a slab would place them by its own
+            raise ValueError("SlabRun implements the heated west wall only (heat='west')")
         self.transport = transport or LocalTransport()
         dist_mode = isinstance(self.transport, DistTransport)
         if dist_mode:

@@ -281,3 +281,14 @@ def test_slab_run_rejects_walls_other_than_no_slip(wall):
     with pytest.raises(ValueError, match="code 4"):
         SlabRun(params, nslabs=2, halo=2, slab_factory=lambda plan, r: made.append(r))
     assert made == []
+
+
+@pytest.mark.parametrize("heat", ["right", "bottom", 3])
+def test_slab_run_rejects_heating_options(heat):
+    """The heating options place the liquid layer and the hot wall by global
+    rows and columns, so SlabRun refuses them before it creates a slab."""
+    from bgk_pcm_b200.slab import SlabRun
+    made = []
+    with pytest.raises(ValueError, match="west"):
+        SlabRun(small_params(12, 16), nslabs=2, halo=2, slab_factory=lambda plan, r: made.append(r), heat=heat)
+    assert made == []
