@@ -605,7 +605,7 @@ def main():
             "metric": METRIC, "value": value, "unit": "GLUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": args.precision,
-            "data": "synthetic: the reference's initial condition on the generated input.dat",
+            "data": "synthetic (the reference's initial condition on the generated input.dat)",
             "config": bench_config(args, params, wl),
             "layout": {"parallelism": (f"yslab{world}" if slab else
                                        (f"replicas{world}" if world > 1 else "single-gpu")),
