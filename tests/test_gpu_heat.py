@@ -203,3 +203,21 @@ def test_heat_snapshot_round_trip_and_mismatch(oracle_mod, lib, tmp_path):
         w.load(tmp_path / "right.bin")
     for x in (w, b, s, o):
         x.close()
+
+
+def test_heat_right_fma_variant_smooth(oracle_mod, lib):
+    """The FMA-contracted FP64 variant runs FROMRIGHT on the same ring path;
+    in the smooth form it stays within max-abs 1e-10 of the oracle."""
+    from bgk_pcm_b200 import Solver
+    p = small_params(80, 30)
+    o = oracle_mod.Oracle(p, tanh="portable", smooth=True, heat=RIGHT)
+    o.initialization()
+    s = Solver(p, tanh="portable", fma=True, smooth=True, heat="right")
+    s.initialization()
+    o.step(60)
+    s.step(60)
+    for name in MACRO:
+        d = np.abs(s.field(name) - o.field(name)).max()
+        assert d <= 1e-10, f"{name}: max-abs {d:.3e}"
+    s.close()
+    o.close()
