@@ -180,7 +180,7 @@ inline const double *east_tcol(const bgk_ctx *c, int buf) { return c->tright ? c
 
 cudaError_t launch_init_f64(bgk_ctx *c);
 cudaError_t launch_bc_prep(bgk_ctx *c);
-cudaError_t launch_ring_bc(bgk_ctx *c);            /* BC_f + BC_g halos, walls other than 4 */
+cudaError_t launch_ring_bc(bgk_ctx *c);            /* BC_f + BC_g halos + bc_prep, walls other than 4 */
 cudaError_t launch_macro_halos(bgk_ctx *c);
 cudaError_t launch_fused_f64(bgk_ctx *c, bool moments);
 cudaError_t launch_flow_f64(bgk_ctx *c, int nsteps);     /* dataflow steps, no moments */

@@ -607,7 +607,6 @@ int bgk_step(bgk_ctx *c, int nsteps)
             /* BC_f and the halo part of BC_g every step, then the west/east
              * g values from this step's velocity halos (STEP_7/BC_g.f90:7-31) */
             CK(bgk::launch_ring_bc(c), "ring boundary");
-            CK(bgk::launch_bc_prep(c), "bc_prep");
         } else if (last) {
             CK(bgk::launch_macro_halos(c), "macro_halos");
         }

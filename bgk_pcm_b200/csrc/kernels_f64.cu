@@ -105,13 +105,11 @@ __global__ void init_kernel(Consts c, int westBC, StepPtrs<double> s, double *fc
  * w_k*T(1,j)*poly of directions 3, 7, 6, T(1,j) being the previous step's
  * (the T mirror, which the ring step writes at edge nodes every step); this
  * then runs before every step. */
-__global__ void bc_prep_kernel(Consts c, const double *mu, const double *mv, const double *mphi,
-                               const double *mT, const double *tin, double *gW, double *pE, double *phiW,
-                               double *phiE)
+__device__ __forceinline__ void bc_prep_row(const Consts &c, const double *mu, const double *mv,
+                                            const double *mphi, const double *mT, const double *tin, double *gW,
+                                            double *pE, double *phiW, double *phiE, int j)
 {
     const int Ny = c.Ny, NX2 = c.Nx + 2;
-    const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    if (j > Ny) return;
     double P[9];
     const size_t qw = (size_t)NX2 * j, qe = (size_t)(c.Nx + 1) + (size_t)NX2 * j;
     eq_poly(mu[qw], mv[qw], P);
@@ -132,6 +130,15 @@ __global__ void bc_prep_kernel(Consts c, const double *mu, const double *mv, con
     pE[2 * Ny + j - 1] = P[7];
     phiW[j - 1] = mphi[qw];
     phiE[j - 1] = mphi[qe];
+}
+
+__global__ void bc_prep_kernel(Consts c, const double *mu, const double *mv, const double *mphi,
+                               const double *mT, const double *tin, double *gW, double *pE, double *phiW,
+                               double *phiE)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (j > c.Ny) return;
+    bc_prep_row(c, mu, mv, mphi, mT, tin, gW, pE, phiW, phiE, j);
 }
 
 /* Halo cells between population rings and reference-layout arrays (pitch
@@ -387,11 +394,12 @@ __global__ void staged_bc_g(Staged s, Consts c)
  * current buffer, halo f in the ring, rho/u/v in the mirrors (which hold the
  * previous step's moments on the edge rows and columns and the reference's
  * halo values).  Then the macroscopic halo assignments of BC_g
- * (STEP_7/BC_g.f90:7-64): T west/east, then T and phi north/south.  One
- * block; the phases are separated by barriers, so each reads what the
- * previous ones wrote, as in the reference.  The g halos themselves are not
- * stored: the step computes them (west and east from bc_prep's per-row
- * values, north and south as copies). */
+ * (STEP_7/BC_g.f90:7-64): T west/east, then T and phi north/south, and
+ * bc_prep's per-row west/east values.  Three launches (ring_k1..k3 below)
+ * keep every phase after the phases whose cells it reads, as in the
+ * reference.  The g halos themselves are not stored: the step computes them
+ * (west and east from bc_prep's per-row values, north and south as
+ * copies). */
 struct RingF {
     const double *fc;      /* compact planes (current buffer) */
     double *ring;
@@ -405,157 +413,226 @@ struct RingF {
     __device__ void set(int k, int i, int j, double v) const { ring[k * RL + ring_idx(Nx, Ny, i, j)] = v; }
 };
 
-__global__ void ring_bc_kernel(Consts c, RingF F, double *rho, double *u, double *v, double *T, double *phi,
-                               const double *tin, const double *tcol, int wbc, int ebc, int nbc, int sbc)
+/* The phases of the boundary update, one cell (row j or column i) per
+ * call, with the reference's formulas and ranges. */
+__device__ __forceinline__ void ring_west(const Consts &c, const RingF &F, double *rho, double *u, double *v,
+                                          int wbc, int j)
 {
     const int Nx = c.Nx, Ny = c.Ny, NX2 = Nx + 2;
     const double *w = c.w;
-    const int t0 = threadIdx.x, nt = blockDim.x;
     double P[9];
-    /* WEST */
     if (wbc == 0) {
-        for (int j = t0; j <= Ny + 1; j += nt)
-            for (int k = 0; k < 9; k++) F.set(k, 0, j, F.get(k, Nx, j));
+        double q[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) q[k] = F.get(k, Nx, j);
+#pragma unroll
+        for (int k = 0; k < 9; k++) F.set(k, 0, j, q[k]);
     } else if (wbc == 1) {
+        if (j < 1 || j > Ny) return;
         eq_poly(c.u0, c.v0, P);
-        for (int j = 1 + t0; j <= Ny; j += nt) {
-            double r = rho[SQ(1, j)];
-            F.set(1, 0, j, w[1] * r * P[1]);
-            F.set(5, 0, j, w[5] * r * P[5]);
-            F.set(8, 0, j, w[8] * r * P[8]);
-            u[SQ(0, j)] = c.u0;
-            v[SQ(0, j)] = c.v0;
-            rho[SQ(0, j)] = rho[SQ(1, j)];
-        }
+        double r = rho[SQ(1, j)];
+        F.set(1, 0, j, w[1] * r * P[1]);
+        F.set(5, 0, j, w[5] * r * P[5]);
+        F.set(8, 0, j, w[8] * r * P[8]);
+        u[SQ(0, j)] = c.u0;
+        v[SQ(0, j)] = c.v0;
+        rho[SQ(0, j)] = rho[SQ(1, j)];
     } else if (wbc == 2) {
-        for (int j = t0; j <= Ny + 1; j += nt) {
-            eq_poly(u[SQ(0, j)], c.v0, P);
-            double r = rho[SQ(1, j)];
-            F.set(1, 0, j, w[1] * r * P[1]);
-            F.set(5, 0, j, w[5] * r * P[5]);
-            F.set(8, 0, j, w[8] * r * P[8]);
-        }
+        eq_poly(u[SQ(0, j)], c.v0, P);
+        double r = rho[SQ(1, j)];
+        F.set(1, 0, j, w[1] * r * P[1]);
+        F.set(5, 0, j, w[5] * r * P[5]);
+        F.set(8, 0, j, w[8] * r * P[8]);
     } else if (wbc == 3) {
-        for (int j = t0; j <= Ny + 1; j += nt) {
-            double u1 = u[SQ(1, j)], v1 = v[SQ(1, j)];
-            eq_poly(u1, v1, P);
-            F.set(1, 0, j, w[1] * c.rho1 * P[1]);
-            F.set(5, 0, j, w[5] * c.rho1 * P[5]);
-            F.set(8, 0, j, w[8] * c.rho1 * P[8]);
-            u[SQ(0, j)] = u1;
-            v[SQ(0, j)] = v1;
-            rho[SQ(0, j)] = c.rho1;
-        }
+        double u1 = u[SQ(1, j)], v1 = v[SQ(1, j)];
+        eq_poly(u1, v1, P);
+        F.set(1, 0, j, w[1] * c.rho1 * P[1]);
+        F.set(5, 0, j, w[5] * c.rho1 * P[5]);
+        F.set(8, 0, j, w[8] * c.rho1 * P[8]);
+        u[SQ(0, j)] = u1;
+        v[SQ(0, j)] = v1;
+        rho[SQ(0, j)] = c.rho1;
     } else if (wbc == 4) {
-        for (int j = 1 + t0; j <= Ny; j += nt) {
-            F.set(1, 0, j, F.get(3, 1, j));
-            F.set(8, 0, j, F.get(6, 1, j - 1));
-            F.set(5, 0, j, F.get(7, 1, j + 1));
-        }
+        if (j < 1 || j > Ny) return;
+        const double a = F.get(3, 1, j), b = F.get(6, 1, j - 1), d = F.get(7, 1, j + 1);
+        F.set(1, 0, j, a);
+        F.set(8, 0, j, b);
+        F.set(5, 0, j, d);
     }
-    __syncthreads();
-    /* EAST */
+}
+
+__device__ __forceinline__ void ring_east(const Consts &c, const RingF &F, double *rho, double *u, double *v,
+                                          int ebc, int j)
+{
+    const int Nx = c.Nx, Ny = c.Ny, NX2 = Nx + 2;
+    const double *w = c.w;
+    double P[9];
     if (ebc == 0) {
-        for (int j = t0; j <= Ny + 1; j += nt)
-            for (int k = 0; k < 9; k++) F.set(k, Nx + 1, j, F.get(k, 1, j));
+        double q[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) q[k] = F.get(k, 1, j);
+#pragma unroll
+        for (int k = 0; k < 9; k++) F.set(k, Nx + 1, j, q[k]);
     } else if (ebc == 3) {
-        for (int j = 1 + t0; j <= Ny; j += nt) {
-            double un = u[SQ(Nx, j)], vn = v[SQ(Nx, j)];
-            eq_poly(un, vn, P);
-            F.set(3, Nx + 1, j, w[3] * c.rho0 * P[3]);
-            F.set(6, Nx + 1, j, w[6] * c.rho0 * P[6]);
-            F.set(7, Nx + 1, j, w[7] * c.rho0 * P[7]);
-            u[SQ(Nx + 1, j)] = un;
-            v[SQ(Nx + 1, j)] = vn;
-            rho[SQ(Nx + 1, j)] = c.rho0;
-        }
+        if (j < 1 || j > Ny) return;
+        double un = u[SQ(Nx, j)], vn = v[SQ(Nx, j)];
+        eq_poly(un, vn, P);
+        F.set(3, Nx + 1, j, w[3] * c.rho0 * P[3]);
+        F.set(6, Nx + 1, j, w[6] * c.rho0 * P[6]);
+        F.set(7, Nx + 1, j, w[7] * c.rho0 * P[7]);
+        u[SQ(Nx + 1, j)] = un;
+        v[SQ(Nx + 1, j)] = vn;
+        rho[SQ(Nx + 1, j)] = c.rho0;
     } else if (ebc == 4) {
-        for (int j = 1 + t0; j <= Ny; j += nt) {
-            F.set(3, Nx + 1, j, F.get(1, Nx, j));
-            F.set(6, Nx + 1, j, F.get(8, Nx, j + 1));
-            F.set(7, Nx + 1, j, F.get(5, Nx, j - 1));
-        }
+        if (j < 1 || j > Ny) return;
+        const double a = F.get(1, Nx, j), b = F.get(8, Nx, j + 1), d = F.get(5, Nx, j - 1);
+        F.set(3, Nx + 1, j, a);
+        F.set(6, Nx + 1, j, b);
+        F.set(7, Nx + 1, j, d);
     }
-    __syncthreads();
-    /* NORTH */
+}
+
+__device__ __forceinline__ void ring_north(const Consts &c, const RingF &F, double *rho, double *u, double *v,
+                                           int nbc, int i)
+{
+    const int Nx = c.Nx, Ny = c.Ny, NX2 = Nx + 2;
+    const double *w = c.w;
+    double P[9];
     if (nbc == 0) {
-        for (int i = t0; i <= Nx + 1; i += nt)
-            for (int k = 0; k < 9; k++) F.set(k, i, Ny + 1, F.get(k, i, 1));
+        double q[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) q[k] = F.get(k, i, 1);
+#pragma unroll
+        for (int k = 0; k < 9; k++) F.set(k, i, Ny + 1, q[k]);
     } else if (nbc == 4) {
-        for (int i = 1 + t0; i <= Nx; i += nt) {
-            F.set(4, i, Ny + 1, F.get(2, i, Ny));
-            F.set(7, i, Ny + 1, F.get(5, i - 1, Ny));
-            F.set(8, i, Ny + 1, F.get(6, i + 1, Ny));
-            rho[SQ(i, Ny + 1)] = rho[SQ(i, Ny)];
-            u[SQ(i, Ny + 1)] = 0.0;
-            v[SQ(i, Ny + 1)] = 0.0;
+        if (i == 0) {
+            F.set(8, 0, Ny + 1, F.get(6, 1, Ny));
+            return;
         }
-        if (t0 == 0) F.set(8, 0, Ny + 1, F.get(6, 1, Ny));
+        if (i > Nx) return;
+        const double a = F.get(2, i, Ny), b = F.get(5, i - 1, Ny), d = F.get(6, i + 1, Ny);
+        F.set(4, i, Ny + 1, a);
+        F.set(7, i, Ny + 1, b);
+        F.set(8, i, Ny + 1, d);
+        rho[SQ(i, Ny + 1)] = rho[SQ(i, Ny)];
+        u[SQ(i, Ny + 1)] = 0.0;
+        v[SQ(i, Ny + 1)] = 0.0;
     } else if (nbc == 5) {
-        for (int i = t0; i <= Nx + 1; i += nt) {
-            F.set(4, i, Ny + 1, F.get(2, i, Ny - 1));
-            F.set(7, i, Ny + 1, F.get(6, i, Ny - 1));
-            F.set(8, i, Ny + 1, F.get(5, i, Ny - 1));
-        }
+        const double a = F.get(2, i, Ny - 1), b = F.get(6, i, Ny - 1), d = F.get(5, i, Ny - 1);
+        F.set(4, i, Ny + 1, a);
+        F.set(7, i, Ny + 1, b);
+        F.set(8, i, Ny + 1, d);
     } else if (nbc == 6) {
-        for (int i = t0; i <= Nx + 1; i += nt) {
-            F.set(4, i, Ny + 1, F.get(4, i, Ny));
-            F.set(7, i, Ny + 1, F.get(7, i, Ny));
-            F.set(8, i, Ny + 1, F.get(8, i, Ny));
-        }
+        const double a = F.get(4, i, Ny), b = F.get(7, i, Ny), d = F.get(8, i, Ny);
+        F.set(4, i, Ny + 1, a);
+        F.set(7, i, Ny + 1, b);
+        F.set(8, i, Ny + 1, d);
     } else if (nbc == 1) {
         eq_poly(c.u0, c.v0, P);
-        for (int i = t0; i <= Nx + 1; i += nt) {
-            double r = rho[SQ(i, Ny)];
-            F.set(4, i, Ny + 1, w[4] * r * P[4]);
-            F.set(7, i, Ny + 1, w[7] * r * P[7]);
-            F.set(8, i, Ny + 1, w[8] * r * P[8]);
-        }
+        double r = rho[SQ(i, Ny)];
+        F.set(4, i, Ny + 1, w[4] * r * P[4]);
+        F.set(7, i, Ny + 1, w[7] * r * P[7]);
+        F.set(8, i, Ny + 1, w[8] * r * P[8]);
     }
-    __syncthreads();
-    /* SOUTH */
+}
+
+__device__ __forceinline__ void ring_south(const Consts &c, const RingF &F, double *rho, double *u, double *v,
+                                           int sbc, int i)
+{
+    const int Nx = c.Nx, Ny = c.Ny, NX2 = Nx + 2;
     if (sbc == 0) {
-        for (int i = t0; i <= Nx + 1; i += nt)
-            for (int k = 0; k < 9; k++) F.set(k, i, 0, F.get(k, i, Ny));
+        double q[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) q[k] = F.get(k, i, Ny);
+#pragma unroll
+        for (int k = 0; k < 9; k++) F.set(k, i, 0, q[k]);
     } else if (sbc == 4) {
-        for (int i = 1 + t0; i <= Nx; i += nt) {
-            F.set(2, i, 0, F.get(4, i, 1));
-            F.set(5, i, 0, F.get(7, i + 1, 1));
-            F.set(6, i, 0, F.get(8, i - 1, 1));
-            rho[SQ(i, 0)] = rho[SQ(i, 1)];
-            u[SQ(i, 0)] = 0.0;
-            v[SQ(i, 0)] = 0.0;
+        if (i == 0) {
+            F.set(5, 0, 0, F.get(7, 1, 1));
+            return;
         }
-        if (t0 == 0) F.set(5, 0, 0, F.get(7, 1, 1));
+        if (i > Nx) return;
+        const double a = F.get(4, i, 1), b = F.get(7, i + 1, 1), d = F.get(8, i - 1, 1);
+        F.set(2, i, 0, a);
+        F.set(5, i, 0, b);
+        F.set(6, i, 0, d);
+        rho[SQ(i, 0)] = rho[SQ(i, 1)];
+        u[SQ(i, 0)] = 0.0;
+        v[SQ(i, 0)] = 0.0;
     } else if (sbc == 6) {
-        for (int i = t0; i <= Nx + 1; i += nt) {
-            F.set(2, i, 0, F.get(2, i, 1));
-            F.set(5, i, 0, F.get(5, i, 1));
-            F.set(6, i, 0, F.get(6, i, 1));
-        }
+        const double a = F.get(2, i, 1), b = F.get(5, i, 1), d = F.get(6, i, 1);
+        F.set(2, i, 0, a);
+        F.set(5, i, 0, b);
+        F.set(6, i, 0, d);
     }
-    __syncthreads();
-    /* BC_g, macroscopic part: T west/east (T(Nx,j) of the previous moments
-     * is tcol; with BGK_HEAT_RIGHT, T(1,j) of the previous step is in the
-     * mirror and the east wall is Tin), then T and phi north/south */
-    for (int j = 1 + t0; j <= Ny; j += nt) {
-        if (c.heat & BGK_HEAT_RIGHT) {
-            T[SQ(0, j)] = T[SQ(1, j)];
-            T[SQ(Nx + 1, j)] = c.Tin;
-        } else {
-            T[SQ(0, j)] = tin ? tin[j - 1] : c.Tin;
-            T[SQ(Nx + 1, j)] = tcol[j - 1];
-        }
+}
+
+/* BC_g's T west/east (T(Nx,j) of the previous moments is tcol; with
+ * BGK_HEAT_RIGHT, T(1,j) of the previous step is in the mirror and the east
+ * wall is Tin), rows j = 1..Ny */
+__device__ __forceinline__ void ring_g_west_east(const Consts &c, double *T, const double *tin, const double *tcol,
+                                                 int j)
+{
+    const int Nx = c.Nx, NX2 = Nx + 2;
+    if (c.heat & BGK_HEAT_RIGHT) {
+        T[SQ(0, j)] = T[SQ(1, j)];
+        T[SQ(Nx + 1, j)] = c.Tin;
+    } else {
+        T[SQ(0, j)] = tin ? tin[j - 1] : c.Tin;
+        T[SQ(Nx + 1, j)] = tcol[j - 1];
     }
-    __syncthreads();
-    for (int i = t0; i <= Nx + 1; i += nt) {
-        T[SQ(i, Ny + 1)] = T[SQ(i, Ny)];
-        phi[SQ(i, Ny + 1)] = phi[SQ(i, Ny)];
-    }
-    __syncthreads();
-    for (int i = t0; i <= Nx + 1; i += nt) {
+}
+
+/* The update runs as three launches; within one, phases that neither read
+ * nor write each other's cells run side by side, one thread per cell.
+ *  1. BC_f west and east.  West writes column 0 and reads columns 1 and Nx;
+ *     east writes column Nx+1 and reads columns 1 and Nx.
+ *  2. BC_f north and south, and BC_g's T west/east.  North writes row Ny+1
+ *     and reads rows Ny-1, Ny and 1; south writes row 0 and reads rows 1
+ *     and Ny; BC_g touches only T, which BC_f neither reads nor writes.  The
+ *     one exception, north code 5 reading row Ny-1 = 0 when Ny = 1, runs
+ *     south as a launch of its own after north.
+ *  3. BC_g's T and phi north (row Ny+1 from row Ny, whose ends step 2
+ *     wrote) and south (row 0 from row 1), and bc_prep's per-row values
+ *     (from the u, v halos of step 1 and the T mirror).
+ * Each launch sees what the previous ones wrote (stream order), as each
+ * phase of the reference sees the phases before it. */
+__global__ void ring_k1(Consts c, RingF F, double *rho, double *u, double *v, int wbc, int ebc)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x, n = c.Ny + 2;
+    if (t < n) ring_west(c, F, rho, u, v, wbc, t);
+    else if (t < 2 * n) ring_east(c, F, rho, u, v, ebc, t - n);
+}
+
+__global__ void ring_k2(Consts c, RingF F, double *rho, double *u, double *v, double *T, const double *tin,
+                        const double *tcol, int nbc, int sbc, bool with_south)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x, m = c.Nx + 2;
+    const int ns = with_south ? m : 0;
+    if (t < m) ring_north(c, F, rho, u, v, nbc, t);
+    else if (t < m + ns) ring_south(c, F, rho, u, v, sbc, t - m);
+    else if (t < m + ns + c.Ny) ring_g_west_east(c, T, tin, tcol, t - m - ns + 1);
+}
+
+__global__ void ring_k2_south(Consts c, RingF F, double *rho, double *u, double *v, int sbc)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < c.Nx + 2) ring_south(c, F, rho, u, v, sbc, t);
+}
+
+__global__ void ring_k3(Consts c, double *T, double *phi, const double *mu, const double *mv, const double *tin,
+                        double *gW, double *pE, double *phiW, double *phiE)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x, m = c.Nx + 2, Ny = c.Ny, NX2 = c.Nx + 2;
+    if (t < m) {
+        T[SQ(t, Ny + 1)] = T[SQ(t, Ny)];
+        phi[SQ(t, Ny + 1)] = phi[SQ(t, Ny)];
+    } else if (t < 2 * m) {
+        const int i = t - m;
         T[SQ(i, 0)] = T[SQ(i, 1)];
         phi[SQ(i, 0)] = phi[SQ(i, 1)];
+    } else if (t < 2 * m + Ny) {
+        bc_prep_row(c, mu, mv, phi, T, tin, gW, pE, phiW, phiE, t - 2 * m + 1);
     }
 }
 
@@ -826,9 +903,16 @@ cudaError_t launch_ring_bc(bgk_ctx *c)
     F.P = c->P;
     F.Nx = c->Nx;
     F.Ny = c->Ny;
-    ring_bc_kernel<<<1, 1024, 0, c->stream>>>(c->c, F, c->mrho, c->mu, c->mv, c->mT, c->mphi, c->tin_rows,
-                                               c->tcol[c->cur], c->p.westBC, c->p.eastBC, c->p.northBC,
-                                               c->p.southBC);
+    const int Nx = c->Nx, Ny = c->Ny, nb = 256;
+    const bool with_south = !(c->p.northBC == 5 && Ny < 2);
+    const int n1 = 2 * (Ny + 2), n2 = (Nx + 2) * (with_south ? 2 : 1) + Ny, n3 = 2 * (Nx + 2) + Ny;
+    ring_k1<<<(n1 + nb - 1) / nb, nb, 0, c->stream>>>(c->c, F, c->mrho, c->mu, c->mv, c->p.westBC, c->p.eastBC);
+    ring_k2<<<(n2 + nb - 1) / nb, nb, 0, c->stream>>>(c->c, F, c->mrho, c->mu, c->mv, c->mT, c->tin_rows,
+                                                      c->tcol[c->cur], c->p.northBC, c->p.southBC, with_south);
+    if (!with_south)
+        ring_k2_south<<<(Nx + 2 + nb - 1) / nb, nb, 0, c->stream>>>(c->c, F, c->mrho, c->mu, c->mv, c->p.southBC);
+    ring_k3<<<(n3 + nb - 1) / nb, nb, 0, c->stream>>>(c->c, c->mT, c->mphi, c->mu, c->mv, c->tin_rows, c->gW, c->pE,
+                                                      c->phiW, c->phiE);
     return cudaGetLastError();
 }
 
