@@ -207,7 +207,10 @@ def e2e_run(params, precision, steps, device, torch, tanh="portable"):
     from bgk_pcm_b200 import Solver
     Nx, Ny = params["Nx"], params["Ny"]
     shape = (Ny + 2, Nx + 2)
-    names = [f"f{k}" for k in range(9)] + [f"g{k}" for k in range(9)] + ["rho", "T", "u", "v", "phi"]
+    # the fields a step reads: the populations, phi, T (its column Nx is the
+    # lagged east wall) and u, v (their halos feed BC_g); rho is recomputed
+    # from the populations before anything reads it
+    names = [f"f{k}" for k in range(9)] + [f"g{k}" for k in range(9)] + ["T", "u", "v", "phi"]
     src = Solver(params, precision=precision, device=device, tanh=tanh)
     src.initialization()
     host_in = {}
@@ -280,12 +283,12 @@ def slab_timed(params, precision, steps, warmup, halo, torch, dist, sampler=None
 
 
 def e2e_slab(params, precision, steps, halo, torch, dist, tanh="portable"):
-    """The end-to-end run of this rank's slab: its initial fields uploaded
-    from pinned host memory, the steps with the diagnostic cadence (sums
+    """The end-to-end run of this rank's slab: the initial fields a step
+    reads (as in e2e_run) uploaded from pinned host memory, the steps with the diagnostic cadence (sums
     all-reduced, the probe read back every 1000 steps), and its
     rho/T/u/v/phi downloaded (the slab's whole reference-layout fields)."""
     from bgk_pcm_b200.slab import DistTransport, SlabRun
-    names = [f"f{k}" for k in range(9)] + [f"g{k}" for k in range(9)] + ["rho", "T", "u", "v", "phi"]
+    names = [f"f{k}" for k in range(9)] + [f"g{k}" for k in range(9)] + ["T", "u", "v", "phi"]
     run = SlabRun(params, halo=halo, precision=precision, transport=DistTransport(), tanh=tanh)
     s = run.slabs[0].solver
     s.initialization()
@@ -585,8 +588,9 @@ def main():
         e_ms = max_over_ranks(e_ms, dist, "cuda")
         e2e = {"value": whole_job_glups(nodes, args.steps, world, e_ms), "unit": "GLUPS",
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-               "what": "initial state (23 reference-layout fields) uploaded from pinned host memory, the steps "
-                       "with field sums + probe read back every 1000 steps, final rho/T/u/v/phi downloaded"}
+               "what": "initial state (the 22 reference-layout fields a step reads: f, g, T, u, v, phi) uploaded "
+                       "from pinned host memory, the steps with field sums + probe read back every 1000 steps, final "
+                       "rho/T/u/v/phi downloaded"}
 
     cpu = cpu1 = None
     if rank == 0 and world == 1 and not args.no_cpu:
