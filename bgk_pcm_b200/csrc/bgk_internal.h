@@ -78,6 +78,7 @@ struct StepPtrs {
     const double *gW;      /* [3][Ny]  g1,g5,g8 west values, row j at j-1   */
     const double *pE;      /* [3][Ny]  east equilibrium polynomials k=3,6,7 */
     const double *phiW, *phiE;   /* [Ny]                                    */
+    const double *tin;     /* per-row hot wall [Ny], or null (scalar Tin)   */
     double *mrho, *mT, *mu, *mv, *mphi;  /* mirrors, or null               */
     const double *ring;    /* f halo ring [9][ring_len] (walls other than 4) */
     long long ring_len;
@@ -182,7 +183,10 @@ cudaError_t launch_init_f64(bgk_ctx *c);
 cudaError_t launch_bc_prep(bgk_ctx *c);
 cudaError_t launch_ring_bc(bgk_ctx *c);            /* BC_f + BC_g halos + bc_prep, walls other than 4 */
 cudaError_t launch_macro_halos(bgk_ctx *c);
-cudaError_t launch_fused_f64(bgk_ctx *c, bool moments);
+/* moments: write rho, T, u, v, phi of every node (the last step of a call);
+ * edge_halos: write instead the halo cells those fields get from this step's
+ * edge nodes (the step before the last of a call, FP64 pipeline only) */
+cudaError_t launch_fused_f64(bgk_ctx *c, bool moments, bool edge_halos = false);
 cudaError_t launch_flow_f64(bgk_ctx *c, int nsteps);     /* dataflow steps, no moments */
 cudaError_t launch_staged(bgk_ctx *c, int stage);   /* 1..8 in main.f90 order */
 cudaError_t launch_compact_to_staged(bgk_ctx *c);
@@ -196,7 +200,7 @@ cudaError_t launch_fused_f64_ptrs(bgk_ctx *c, const double *fin, const double *g
                                   const double *tcin, double *fout, double *gout, double *phout, double *tcout);
 
 /* kernels_fast.cu (FMA allowed): FP64-FMA, FP32 and FP16 forms */
-cudaError_t launch_fused_fast(bgk_ctx *c, bool moments);
+cudaError_t launch_fused_fast(bgk_ctx *c, bool moments, bool edge_halos = false);
 cudaError_t launch_init_lowp(bgk_ctx *c);
 cudaError_t launch_flow_lowp(bgk_ctx *c, int nsteps);   /* dataflow steps, no moments */
 cudaError_t launch_flow_fast(bgk_ctx *c, int nsteps);   /* FMA FP64 or reduced precision */

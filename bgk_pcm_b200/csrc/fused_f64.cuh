@@ -46,10 +46,42 @@ __device__ __forceinline__ void prefetch_row(const T *F, const T *G, const TP *P
  * forces, collision, stores and (when required) moments.  Shared by the
  * register-pull kernel below and the shared-memory pipeline kernel
  * (fused_pipe.cuh), so both round identically. */
-template <int TANH, bool MOM, bool REF32, bool RING = false>
+/* The halo cells of rho, T, u, v and phi that STEP_7's BC_f (code 4) and
+ * BC_g copy from the edge nodes at the start of a step
+ * (STEP_7/BC_f.f90:127-134,183-190, BC_g.f90:7-64), written by the edge
+ * node (x, y) of the step before: rm, Tm, phn are its moments.  After the
+ * last step of a call the reference's arrays hold these lagged halos. */
+__device__ __forceinline__ void edge_halos_f64(const StepPtrs<double> &s, const Consts &c, int x, int y, bool W,
+                                               bool E, bool S, bool N, double rm, double Tm, double phn)
+{
+    const int Nx = c.Nx, Ny = c.Ny, i = x + 1, j = y + 1;
+    const size_t X = (size_t)s.NX2;
+    if (N) {
+        const size_t q = (size_t)i + X * (size_t)(Ny + 1);
+        s.mrho[q] = rm; s.mu[q] = 0.0; s.mv[q] = 0.0; s.mT[q] = Tm; s.mphi[q] = phn;
+    }
+    if (S) {
+        const size_t q = (size_t)i;
+        s.mrho[q] = rm; s.mu[q] = 0.0; s.mv[q] = 0.0; s.mT[q] = Tm; s.mphi[q] = phn;
+    }
+    if (E) {
+        s.mT[(size_t)(Nx + 1) + X * (size_t)j] = Tm;
+        if (N) { s.mT[(size_t)(Nx + 1) + X * (size_t)(Ny + 1)] = Tm; s.mphi[(size_t)(Nx + 1) + X * (size_t)(Ny + 1)] = s.phiE[Ny - 1]; }
+        if (S) { s.mT[(size_t)(Nx + 1)] = Tm; s.mphi[(size_t)(Nx + 1)] = s.phiE[0]; }
+    }
+    if (W) {
+        const double tw = s.tin ? s.tin[y] : c.Tin;
+        s.mT[X * (size_t)j] = tw;
+        if (N) { s.mT[X * (size_t)(Ny + 1)] = tw; s.mphi[X * (size_t)(Ny + 1)] = s.phiW[Ny - 1]; }
+        if (S) { s.mT[0] = tw; s.mphi[0] = s.phiW[0]; }
+    }
+}
+
+template <int TANH, bool MOM, bool REF32, bool RING = false, bool EH = false>
 __device__ __forceinline__ void node_f64(const StepPtrs<double> &s, const Consts &c, int x, int y, long long cc,
                                          bool E, double *f, double *g, const double (&ap)[3][3],
-                                         const double (&am)[3][3], const double *pc, bool edge = false)
+                                         const double (&am)[3][3], const double *pc, bool edge = false,
+                                         bool W = false, bool S = false, bool N = false)
 {
     const long long pl = s.plane;
     /* momentsPre */
@@ -91,9 +123,11 @@ __device__ __forceinline__ void node_f64(const StepPtrs<double> &s, const Consts
      * other than code 4, every edge node every step: the next step's BC_f
      * reads rho, u and v there) */
     const bool wm = MOM || (RING && edge);
-    if (wm || E) {
+    const bool eh = EH && edge;
+    if (wm || E || eh) {
         const double Tm = (sum9(out) + T2) * 0.5;
         if (E) s.tcout[y] = Tm;
+        if (eh) edge_halos_f64(s, c, x, y, W, E, S, N, sum9(f), Tm, phn);
         if (wm) {
             const double rm = sum9(f);
             const double irm = 1.0 / rm;

@@ -96,7 +96,7 @@ __device__ __forceinline__ void f64_window_start(const StepPtrs<double> &s, int 
 /* f64_row: node (x, y) from a filled stage -- the window's new row y+1,
  * the pulls (bounce-back, or the halo ring with other wall codes, and the
  * g boundary values), node_f64, and the window shift. */
-template <int TANH, bool MOM, bool REF32, bool RING>
+template <int TANH, bool MOM, bool REF32, bool RING, bool EH = false>
 __device__ __forceinline__ void f64_row(const StepPtrs<double> &s, const Consts &c, const double *__restrict__ corner,
                                         const unsigned char *stage, int x, int y, int tid, bool W, bool E,
                                         double (&ap)[3][3], double (&am)[3][3], double *pc)
@@ -179,7 +179,7 @@ __device__ __forceinline__ void f64_row(const StepPtrs<double> &s, const Consts 
         g[6] = sg[6 * Gm::RW + col + 1];
         g[7] = sg[7 * Gm::RW + col + 1];
     }
-    node_f64<TANH, MOM, REF32, RING>(s, c, x, y, cc, E, f, g, ap, am, pc, W || E || S || N);
+    node_f64<TANH, MOM, REF32, RING, EH>(s, c, x, y, cc, E, f, g, ap, am, pc, W || E || S || N, W, S, N);
 #pragma unroll
     for (int k = 0; k < 3; k++) {
         ap[0][k] = ap[1][k]; ap[1][k] = ap[2][k];
@@ -234,7 +234,7 @@ __device__ __forceinline__ void f64_window_stage(const StepPtrs<double> &s, int 
     }
 }
 
-template <int D, int TANH, bool MOM, bool REF32, bool RING = false>
+template <int D, int TANH, bool MOM, bool REF32, bool RING = false, bool EH = false>
 __global__ void __launch_bounds__(PIPE_THREADS, 3)
 fused_pipe_f64_kernel(StepPtrs<double> s, Consts c, const double *__restrict__ corner, PipeSched sch, int *errflag)
 {
@@ -300,8 +300,8 @@ fused_pipe_f64_kernel(StepPtrs<double> s, Consts c, const double *__restrict__ c
                 break;
             }
             if (active)
-                f64_row<TANH, MOM, REF32, RING>(s, c, corner, stages + (size_t)st * Gm::STAGE_BYTES, x, y, tid, W, E,
-                                                ap, am, pc);
+                f64_row<TANH, MOM, REF32, RING, EH>(s, c, corner, stages + (size_t)st * Gm::STAGE_BYTES, x, y, tid, W,
+                                                    E, ap, am, pc);
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[st]);
             r++;
@@ -478,13 +478,13 @@ inline cudaError_t launch_flow_pipe_f64(bgk_ctx *c, const StepPtrs<double> &s0, 
                  : flow_f64_launch_t<BGK_TANH_DEVICE, false>(c, s0, s1, nsteps);
 }
 
-template <int D, int T, bool M, bool R, bool RING = false>
+template <int D, int T, bool M, bool R, bool RING = false, bool EH = false>
 inline cudaError_t pipe_f64_launch(const bgk_ctx *c, const StepPtrs<double> &s, int ctas)
 {
     using Gm = PipeGeom<double, double>;
     const size_t smem = Gm::smem_bytes(D);
     static std::atomic<unsigned long long> done{0};
-    const cudaError_t e = pipe_configure(fused_pipe_f64_kernel<D, T, M, R, RING>, smem, c->dev, done);
+    const cudaError_t e = pipe_configure(fused_pipe_f64_kernel<D, T, M, R, RING, EH>, smem, c->dev, done);
     if (e != cudaSuccess) return e;
     int grid;
     const PipeSched sch = pipe_sched(c, ctas, 4, &grid, 32);
@@ -492,10 +492,10 @@ inline cudaError_t pipe_f64_launch(const bgk_ctx *c, const StepPtrs<double> &s, 
      * steps are short enough (tens of microseconds) for the launch gap to
      * matter: +9 % at 512^2; on larger grids it measured ~1 % slower */
     if ((long long)c->Nx * c->Ny <= (1LL << 21))
-        return pdl_launch(fused_pipe_f64_kernel<D, T, M, R, RING>, grid, PIPE_THREADS, smem, c->stream, s, c->c,
+        return pdl_launch(fused_pipe_f64_kernel<D, T, M, R, RING, EH>, grid, PIPE_THREADS, smem, c->stream, s, c->c,
                           (const double *)c->corner, sch, c->errflag);
-    fused_pipe_f64_kernel<D, T, M, R, RING><<<grid, PIPE_THREADS, smem, c->stream>>>(s, c->c, c->corner, sch,
-                                                                                   c->errflag);
+    fused_pipe_f64_kernel<D, T, M, R, RING, EH><<<grid, PIPE_THREADS, smem, c->stream>>>(s, c->c, c->corner, sch,
+                                                                                       c->errflag);
     return cudaGetLastError();
 }
 
@@ -517,10 +517,17 @@ inline cudaError_t pipe_f64_ring_dispatch(const bgk_ctx *c, const StepPtrs<doubl
 }
 
 template <int D>
-inline cudaError_t pipe_f64_dispatch(const bgk_ctx *c, const StepPtrs<double> &s, bool mom, int ctas)
+inline cudaError_t pipe_f64_dispatch(const bgk_ctx *c, const StepPtrs<double> &s, bool mom, int ctas, bool eh)
 {
     const bool portable = c->opt.tanh_mode == BGK_TANH_PORTABLE;
     const bool ref32 = !c->opt.smooth;
+    if (eh && !mom) {
+        if (portable)
+            return ref32 ? pipe_f64_launch<D, BGK_TANH_PORTABLE, false, true, false, true>(c, s, ctas)
+                         : pipe_f64_launch<D, BGK_TANH_PORTABLE, false, false, false, true>(c, s, ctas);
+        return ref32 ? pipe_f64_launch<D, BGK_TANH_DEVICE, false, true, false, true>(c, s, ctas)
+                     : pipe_f64_launch<D, BGK_TANH_DEVICE, false, false, false, true>(c, s, ctas);
+    }
     if (portable) {
         if (mom) return ref32 ? pipe_f64_launch<D, BGK_TANH_PORTABLE, true, true>(c, s, ctas)
                               : pipe_f64_launch<D, BGK_TANH_PORTABLE, true, false>(c, s, ctas);
@@ -537,15 +544,15 @@ inline cudaError_t pipe_f64_dispatch(const bgk_ctx *c, const StepPtrs<double> &s
  * 4096^2: 2 stages with 3 CTAs per SM (12 consumer warps) is best (92 % /
  * 88 % of the copy bandwidth); more stages or CTAs lose occupancy or issue
  * slots. */
-inline cudaError_t launch_fused_pipe_f64(const bgk_ctx *c, const StepPtrs<double> &s, bool mom)
+inline cudaError_t launch_fused_pipe_f64(const bgk_ctx *c, const StepPtrs<double> &s, bool mom, bool eh = false)
 {
     if (c->ring) return pipe_f64_ring_dispatch(c, s, mom, c->tune_ctas > 0 ? c->tune_ctas : 3);
     const int D = c->tune_D > 0 ? c->tune_D : 2;
     const int ctas = c->tune_ctas > 0 ? c->tune_ctas : (D <= 2 ? 3 : 2);
     switch (D) {
-    case 2: return pipe_f64_dispatch<2>(c, s, mom, ctas);
-    case 4: return pipe_f64_dispatch<4>(c, s, mom, ctas);
-    default: return pipe_f64_dispatch<3>(c, s, mom, ctas);
+    case 2: return pipe_f64_dispatch<2>(c, s, mom, ctas, eh);
+    case 4: return pipe_f64_dispatch<4>(c, s, mom, ctas, eh);
+    default: return pipe_f64_dispatch<3>(c, s, mom, ctas, eh);
     }
 }
 

@@ -969,7 +969,7 @@ cudaError_t launch_flow_f64(bgk_ctx *c, int nsteps)
     return launch_flow_pipe_f64(c, s0, s1, nsteps);
 }
 
-cudaError_t launch_fused_f64(bgk_ctx *c, bool moments)
+cudaError_t launch_fused_f64(bgk_ctx *c, bool moments, bool edge_halos)
 {
     StepPtrs<double> s{};
     const int src = c->cur, dst = c->cur ^ 1;
@@ -977,14 +977,14 @@ cudaError_t launch_fused_f64(bgk_ctx *c, bool moments)
     s.fout = (double *)c->fbuf[dst]; s.gout = (double *)c->gbuf[dst];
     s.phin = (const double *)c->phibuf[src]; s.phout = (double *)c->phibuf[dst];
     s.tcin = east_tcol(c, src); s.tcout = c->tcol[dst];
-    s.gW = c->gW; s.pE = c->pE; s.phiW = c->phiW; s.phiE = c->phiE;
+    s.gW = c->gW; s.pE = c->pE; s.phiW = c->phiW; s.phiE = c->phiE; s.tin = c->tin_rows;
     s.mrho = c->mrho; s.mT = c->mT; s.mu = c->mu; s.mv = c->mv; s.mphi = c->mphi;
     s.plane = c->plane; s.P = c->P; s.NX2 = c->NX2;
     s.ring = c->fring; s.ring_len = c->ring_len;
     const int H = strip_height(c);
     dim3 grd((c->Nx + FUSED_BX - 1) / FUSED_BX, (c->Ny + H - 1) / H);
     /* walls other than code 4 run on the pipeline kernel only */
-    if (c->tune_pipe || c->ring) return launch_fused_pipe_f64(c, s, moments);
+    if (c->tune_pipe || c->ring) return launch_fused_pipe_f64(c, s, moments, edge_halos);
     return launch_fused_f64_variant(c, grd, s, H, moments);
 }
 
