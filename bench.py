@@ -189,6 +189,23 @@ def whole_job_glups(nodes: int, steps: int, world: int, ms_max: float) -> float:
     return nodes * steps * world / (ms_max / 1e3) / 1e9
 
 
+def gpu_primer(torch, seconds: float = 0.3) -> None:
+    """Keep the GPU busy with device-to-device copies for `seconds` while the
+    clock sampler starts.  On B200 the first ~10 ms of load after an idle
+    period run ~1 % slower (measured: the first two 20-step calls after 5
+    warm-up steps at 18.6 GLUPS, the next ones and any after 50 warm-up
+    steps at 18.8), which a 20-step window would otherwise carry.  The copies
+    touch no data of the run and end before the warm-up steps."""
+    a = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    b = torch.empty_like(a)
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        for _ in range(8):
+            b.copy_(a)
+        torch.cuda.synchronize()
+    del a, b
+
+
 def time_steps(solver, steps: int, torch):
     stream = torch.cuda.ExternalStream(solver.stream)
     start = torch.cuda.Event(enable_timing=True)
@@ -261,7 +278,7 @@ def slab_timed(params, precision, steps, warmup, halo, torch, dist, sampler=None
     clocks = None
     if sampler:
         sampler.start()
-        time.sleep(0.3)
+        gpu_primer(torch)
     # warm-up right before the timed steps (no idle gap between them)
     run.step(warmup)
     run.sync()
@@ -441,6 +458,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--precision-errors", type=int, default=1,
                     help="1: run the precision workload in full (FP64 and FP32) and report the FP32 form's errors")
+    ap.add_argument("--sustained", type=int, default=10000,
+                    help="steps of one more run of the headline form, timed with its clocks (the power-capped "
+                         "sustained rate; 0 skips it)")
     ap.add_argument("--decomp", default="slab", choices=["slab", "replicas"],
                     help="N > 1: y-slab decomposition of one N-times taller cavity, or N replicas")
     ap.add_argument("--halo", type=int, default=8, help="ghost rows per cut (steps between exchanges)")
@@ -487,9 +507,9 @@ def main():
         sampler = ClockSampler(local) if sample_clocks else None
         if sampler:
             sampler.start()
-            time.sleep(0.3)
+            gpu_primer(torch)
         # the warm-up runs right before the timed steps, so the GPU does not
-        # sit idle (while the clock sampler starts) between the two
+        # sit idle between the two
         s.step(warmup)
         s.sync()
         barrier()
@@ -553,6 +573,15 @@ def main():
             forms[form]["max_abs_vs_headline"] = fp64_divergence(params, local, args.tanh, tanh, fma)
 
     # the precision-form workload (4096^2, Ra 1e7): FP32 storage against FP64
+    # the same form over a long run: a 20-step window runs at the burst
+    # clocks, a run of seconds at the clocks the 1000 W power cap leaves
+    sustained = None
+    if world == 1 and args.sustained and args.sustained > args.steps:
+        sms, sclk = run_form(args.precision, False, args.sustained, args.warmup, sample_clocks=True)
+        sg = nodes * args.sustained / (sms / 1e3) / 1e9
+        sustained = {"steps": args.sustained, "glups": sg, "hbm_gbs": sg * bpn, "frac_of_measured_hbm": sg * bpn / hbm,
+                     "clocks": sclk}
+
     precision_cfg = None
     if world == 1 and "f32" in args.forms.split(",") and args.precision == "f64":
         pwl = "cavity4096_ra1e7"
@@ -620,6 +649,7 @@ def main():
                          "frac": achieved / hbm, "traffic": traffic, "peak_kind": hbm_kind,
                          "bytes_per_node": bpn},
             "forms": forms,
+            "sustained": sustained,
             "precision_config": precision_cfg,
             "adjoint": adjoint,
             "clocks": clocks,

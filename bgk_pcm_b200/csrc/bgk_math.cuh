@@ -149,6 +149,13 @@ BGK_HD double phi_update(const Consts &c, double kp, double km, double th, doubl
     return p0 + (c.f_plus * kp * (1.0 - p0) - c.f_minus * km * (1.0 + p0));
 }
 
+/* x / y for y > 0, skipping the division when x is a zero: 0 / y is that
+ * zero with its sign, bit for bit.  Where the liquid fraction is 1 (and
+ * wherever u is exactly 0, as in the symmetric bulk of the cavity) the drag
+ * numerator is +-0; on B200 a warp whose lanes divide zeros runs the
+ * division measurably slower, so those lanes sit the division out. */
+BGK_HD double div_pos(double x, double y) { return x == 0.0 ? x : x / y; }
+
 /* forces.f90:15-27: latent heat on T, buoyancy + drag, velocity shift. */
 BGK_HD void apply_forces(const Consts &c, double phi, double phip, double rho,
                          double &T, double &u, double &v)
@@ -157,8 +164,9 @@ BGK_HD void apply_forces(const Consts &c, double phi, double phip, double rho,
     double forceY = rho * c.grav * c.beta * T * (1.0 + phi / 2.0);
     double forceX = -(u * (1.0 - phi) * 0.5);
     forceY = forceY - v * (1.0 - phi) * 0.5;
-    u = u + forceX / (c.omega_f * rho);
-    v = v + forceY / (c.omega_f * rho);
+    /* omega_f * rho > 0 (rho is a sum of positive populations) */
+    u = u + div_pos(forceX, c.omega_f * rho);
+    v = v + div_pos(forceY, c.omega_f * rho);
 }
 
 } // namespace bgk
