@@ -189,23 +189,6 @@ def whole_job_glups(nodes: int, steps: int, world: int, ms_max: float) -> float:
     return nodes * steps * world / (ms_max / 1e3) / 1e9
 
 
-def gpu_primer(torch, seconds: float = 0.3) -> None:
-    """Keep the GPU busy with device-to-device copies for `seconds` while the
-    clock sampler starts.  On B200 the first ~10 ms of load after an idle
-    period run ~1 % slower (measured: the first two 20-step calls after 5
-    warm-up steps at 18.6 GLUPS, the next ones and any after 50 warm-up
-    steps at 18.8), which a 20-step window would otherwise carry.  The copies
-    touch no data of the run and end before the warm-up steps."""
-    a = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    b = torch.empty_like(a)
-    t0 = time.perf_counter()
-    while time.perf_counter() - t0 < seconds:
-        for _ in range(8):
-            b.copy_(a)
-        torch.cuda.synchronize()
-    del a, b
-
-
 def time_steps(solver, steps: int, torch):
     stream = torch.cuda.ExternalStream(solver.stream)
     start = torch.cuda.Event(enable_timing=True)
@@ -278,7 +261,7 @@ def slab_timed(params, precision, steps, warmup, halo, torch, dist, sampler=None
     clocks = None
     if sampler:
         sampler.start()
-        gpu_primer(torch)
+        time.sleep(0.3)
     # warm-up right before the timed steps (no idle gap between them)
     run.step(warmup)
     run.sync()
@@ -507,9 +490,9 @@ def main():
         sampler = ClockSampler(local) if sample_clocks else None
         if sampler:
             sampler.start()
-            gpu_primer(torch)
+            time.sleep(0.3)
         # the warm-up runs right before the timed steps, so the GPU does not
-        # sit idle between the two
+        # sit idle (while the clock sampler starts) between the two
         s.step(warmup)
         s.sync()
         barrier()
