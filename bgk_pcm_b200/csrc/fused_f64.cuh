@@ -42,10 +42,6 @@ __device__ __forceinline__ void prefetch_row(const T *F, const T *G, const TP *P
     prefetch_l2(ptr, bytes);
 }
 
-/* One node of the fused step after its pulls: momentsPre, phase_field,
- * forces, collision, stores and (when required) moments.  Shared by the
- * register-pull kernel below and the shared-memory pipeline kernel
- * (fused_pipe.cuh), so both round identically. */
 /* The halo cells of rho, T, u, v and phi that STEP_7's BC_f (code 4) and
  * BC_g copy from the edge nodes at the start of a step
  * (STEP_7/BC_f.f90:127-134,183-190, BC_g.f90:7-64), written by the edge
@@ -77,6 +73,10 @@ __device__ __forceinline__ void edge_halos_f64(const StepPtrs<double> &s, const 
     }
 }
 
+/* One node of the fused step after its pulls: momentsPre, phase_field,
+ * forces, collision, stores and (when required) moments.  Shared by the
+ * register-pull kernel below and the shared-memory pipeline kernel
+ * (fused_pipe.cuh), so both round identically. */
 template <int TANH, bool MOM, bool REF32, bool RING = false, bool EH = false>
 __device__ __forceinline__ void node_f64(const StepPtrs<double> &s, const Consts &c, int x, int y, long long cc,
                                          bool E, double *f, double *g, const double (&ap)[3][3],
