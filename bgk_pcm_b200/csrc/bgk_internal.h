@@ -148,6 +148,11 @@ struct bgk_ctx {
     double *scratch;       /* A doubles                                     */
     double *red;           /* reduction partials; red[0..3] = results        */
     double *corner;        /* f6(Nx+1,0), f7(Nx+1,Ny+1) (never written by BC_f) */
+    /* launch-bound grids (up to 2^21 nodes): the plain steps of a call
+     * replay a captured CUDA graph of GRAPH_STEPS steps, one per starting
+     * buffer (BGK_GRAPH=0 disables) */
+    cudaGraphExec_t step_graph[2];
+    bool graph_on, graph_failed;
     bool ring;             /* a wall other than code 4: f halos in fring     */
     double *fring;         /* [9][ring_len] f halo cells (ring_idx), or null */
     long long ring_len;

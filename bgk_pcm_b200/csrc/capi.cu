@@ -384,6 +384,61 @@ int bgk_read_input(const char *path, bgk_params *out)
         if (e_ != cudaSuccess) { bgk_destroy(c); return cuda_fail(e_, what); } \
     } while (0)
 
+/* ------------------------------------------------------ step graphs */
+
+/* Steps per captured graph: even, so a replay ends on the buffer it starts
+ * from. */
+constexpr int GRAPH_STEPS = 32;
+
+static void drop_step_graphs(bgk_ctx *c)
+{
+    for (int b = 0; b < 2; b++)
+        if (c->step_graph[b]) {
+            cudaGraphExecDestroy(c->step_graph[b]);
+            c->step_graph[b] = nullptr;
+        }
+}
+
+/* One plain step (no moments): the halo-ring update first where it applies. */
+static cudaError_t launch_plain_step(bgk_ctx *c, bool exact)
+{
+    if (c->ring) {
+        cudaError_t e = bgk::launch_ring_bc(c);
+        if (e != cudaSuccess) return e;
+    }
+    return exact ? bgk::launch_fused_f64(c, false) : bgk::launch_fused_fast(c, false);
+}
+
+/* Capture GRAPH_STEPS plain steps starting from buffer c->cur into
+ * c->step_graph[c->cur].  Every kernel involved has been launched once
+ * before (its attributes are set), so the capture holds kernel launches
+ * only.  Returns false (and leaves graphs off for the context) on failure. */
+static bool capture_step_graph(bgk_ctx *c, bool exact)
+{
+    const int start = c->cur;
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < GRAPH_STEPS && e == cudaSuccess; k++) {
+        e = launch_plain_step(c, exact);
+        c->cur ^= 1;
+    }
+    const cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+    c->cur = start;
+    cudaGraphExec_t x = nullptr;
+    if (e == cudaSuccess && e2 == cudaSuccess && g && cudaGraphInstantiate(&x, g, 0) == cudaSuccess) {
+        c->step_graph[start] = x;
+    } else {
+        x = nullptr;
+    }
+    if (g) cudaGraphDestroy(g);
+    (void)cudaGetLastError();
+    return x != nullptr;
+}
+
 int bgk_create(const bgk_params *pp, const bgk_options *opt, bgk_ctx **out)
 {
     if (!pp || !out) return fail(BGK_ERR_ARG, "null argument");
@@ -455,6 +510,10 @@ int bgk_create(const bgk_params *pp, const bgk_options *opt, bgk_ctx **out)
     if (const char *v = getenv("BGK_PIPE_CTAS")) c->tune_ctas = atoi(v);
     c->tune_flow = 0;
     if (const char *v = getenv("BGK_FLOW")) c->tune_flow = atoi(v);
+    c->step_graph[0] = c->step_graph[1] = nullptr;
+    c->graph_failed = false;
+    c->graph_on = (long long)pp->Nx * pp->Ny <= (1LL << 21);
+    if (const char *v = getenv("BGK_GRAPH")) c->graph_on = c->graph_on && atoi(v) != 0;
     c->flow_stall = 0;
     if (const char *v = getenv("BGK_FLOW_STALL")) c->flow_stall = atoi(v) == 1;
     {
@@ -539,6 +598,7 @@ int bgk_destroy(bgk_ctx *c)
         if (c->sfp[k]) cudaFree(c->sfp[k]);
         if (c->sgp[k]) cudaFree(c->sgp[k]);
     }
+    drop_step_graphs(c);
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->adj_ws) cudaFree(c->adj_ws);
     free(c->tin_host);
@@ -552,6 +612,7 @@ int bgk_initialize(bgk_ctx *c)
     if (!c) return fail(BGK_ERR_ARG, "null context");
     int rc = set_device(c);
     if (rc) return rc;
+    drop_step_graphs(c);   /* the reduced-precision scales are set anew */
     c->cur = 0;
     c->mode = 0;
     if (c->opt.precision == BGK_PREC_F64) {
@@ -599,6 +660,24 @@ int bgk_step(bgk_ctx *c, int nsteps)
             done += n;
         }
         t = nflow;
+    }
+    /* Launch-bound grids: the plain steps before the last two as replays of
+     * a captured graph (the kernels and their order are those of the loop
+     * below, so the results are the same bit for bit) */
+    if (c->graph_on && !c->graph_failed && !c->tune_flow && nsteps - 2 - t >= GRAPH_STEPS + 1) {
+        if (!c->step_graph[c->cur ^ 1] || !c->step_graph[c->cur]) {
+            /* one step launched directly first sets every kernel's attributes */
+            CK(launch_plain_step(c, exact), "fused step");
+            c->cur ^= 1;
+            c->it += 1;
+            t += 1;
+            if (!c->step_graph[c->cur] && !capture_step_graph(c, exact)) c->graph_failed = true;
+        }
+        while (!c->graph_failed && c->step_graph[c->cur] && nsteps - 2 - t >= GRAPH_STEPS) {
+            CK(cudaGraphLaunch(c->step_graph[c->cur], c->stream), "step graph");
+            c->it += GRAPH_STEPS;
+            t += GRAPH_STEPS;
+        }
     }
     /* The reference's arrays after the call: the last step's moments, with
      * halos copied from the step before (STEP_7/BC_f.f90, BC_g.f90).  On the
@@ -801,6 +880,7 @@ int bgk_set_tin(bgk_ctx *c, const double *tin, int ny)
     if (!c) return fail(BGK_ERR_ARG, "null context");
     int rc = set_device(c);
     if (rc) return rc;
+    drop_step_graphs(c);   /* the halo-ring update reads the tin pointer */
     if (!tin) {
         if (c->tin_rows) { cudaFree(c->tin_rows); c->tin_rows = nullptr; }
         free(c->tin_host);
@@ -895,6 +975,7 @@ int bgk_load(bgk_ctx *c, const char *path)
     if (!c || !path) return fail(BGK_ERR_ARG, "null argument");
     int rc = set_device(c);
     if (rc) return rc;
+    drop_step_graphs(c);   /* the snapshot may carry other scales or a tin */
     FILE *fp = fopen(path, "rb");
     if (!fp) return fail(BGK_ERR_IO, "cannot read %s", path);
     char mg[8];
