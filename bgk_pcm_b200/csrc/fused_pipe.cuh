@@ -487,7 +487,7 @@ inline cudaError_t pipe_f64_launch(const bgk_ctx *c, const StepPtrs<double> &s, 
     const cudaError_t e = pipe_configure(fused_pipe_f64_kernel<D, T, M, R, RING, EH>, smem, c->dev, done);
     if (e != cudaSuccess) return e;
     int grid;
-    const PipeSched sch = pipe_sched(c, ctas, 4, &grid, 32);
+    const PipeSched sch = pipe_sched(c, ctas, 4, &grid, 32, 2);
     /* programmatic dependent launch on grids of up to 2^21 nodes, whose
      * steps are short enough (tens of microseconds) for the launch gap to
      * matter: +9 % at 512^2; on larger grids it measured ~1 % slower */

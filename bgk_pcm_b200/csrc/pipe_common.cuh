@@ -118,15 +118,17 @@ struct PipeIter {
     }
 };
 
-/* Tile height: max_H rows, halved down to base_H while there are fewer
+/* Tile height: max_H rows, halved down to min_H while there are fewer
  * than 10 tiles per resident CTA, then down to 1 while there are fewer than
  * 4 (small grids, e.g. 512^2 runs best at H = 1).  Taller tiles start fewer
  * phase-field windows and pipeline fills; shorter ones leave a smaller
- * partial last wave.  Measured on B200 (FP64, 200 steps): max_H = 32 gives
- * H = 4 at 2048^2 (18.9 GLUPS; 8/16/32: 18.6/17.8/16.5), 16 at 3072^2 and
- * 4096^2 (+1.5 %, +2.7 % over H = 4) and 32 at 16384x4096 (+2.6 %); the
- * reduced-precision forms run best at H = 8 throughout (max_H = base_H). */
-inline PipeSched pipe_sched(const bgk_ctx *c, int ctas_per_sm, int base_H, int *grid, int max_H = 0)
+ * partial last wave.  Measured on B200 (FP64, 200-1000 steps): max_H = 32,
+ * min_H = 2 give H = 2 at 1024^2 (17.0 GLUPS against 16.2 with H = 4), 4 at
+ * 2048^2 (18.9; 8/16/32: 18.6/17.8/16.5), 16 at 3072^2 and 4096^2 (+1.5 %,
+ * +2.7 % over H = 4) and 32 at 16384x4096 (+2.6 %); the reduced-precision
+ * forms run best at H = 8 throughout (no max_H: H starts at base_H). */
+inline PipeSched pipe_sched(const bgk_ctx *c, int ctas_per_sm, int base_H, int *grid, int max_H = 0,
+                            int min_H = 0)
 {
     PipeSched sch{};
     sch.bx = PIPE_BX;
@@ -134,7 +136,8 @@ inline PipeSched pipe_sched(const bgk_ctx *c, int ctas_per_sm, int base_H, int *
     const long long slots = (long long)c->nsm * ctas_per_sm;
     auto tiles = [&](int h) { return (long long)sch.nbands * ((c->Ny + h - 1) / h); };
     int H = max_H > base_H ? max_H : base_H;
-    while (H > base_H && tiles(H) < 10 * slots) H /= 2;
+    const int lo = min_H > 0 ? min_H : base_H;
+    while (H > lo && tiles(H) < 10 * slots) H /= 2;
     while (H > 1 && tiles(H) < 4 * slots) H /= 2;
     if (c->tune_H > 0) H = c->tune_H;
     sch.H = H;
