@@ -221,3 +221,19 @@ def test_heat_right_fma_variant_smooth(oracle_mod, lib):
         assert d <= 1e-10, f"{name}: max-abs {d:.3e}"
     s.close()
     o.close()
+
+
+@pytest.mark.parametrize("heat,walls", [(RIGHT, (4, 4, 4, 4)), (BOTTOM, (4, 4, 4, 4)), (RIGHT | BOTTOM, (4, 4, 4, 4)),
+                                        (RIGHT, (2, 0, 4, 6))])
+def test_heat_options_long_run_bit_exact(oracle_mod, lib, heat, walls):
+    """2000 steps in calls of 1000 (the plain steps replay captured step
+    graphs on this grid, through the halo-ring update for FROMRIGHT): every
+    array still equals the oracle bit for bit."""
+    o, s = _pair(oracle_mod, 200, 96, heat, walls)
+    ring = bool(heat & RIGHT) or walls != (4, 4, 4, 4)
+    for _ in range(2):
+        o.step(1000)
+        s.step(1000)
+    _assert_equal(o, s, f"heat {heat} walls {walls} after 2000 steps", f_halos=ring)
+    s.close()
+    o.close()
