@@ -931,9 +931,9 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
     bool binomial = spec->checkpoint_every < 0 || (size_t)(nsnap + K + 1) * state_bytes > avail;
     int nslots = 0;                        /* binomial: state slots incl. S(0) */
     if (binomial) {
-        nslots = spec->checkpoint_every < 0 ? -spec->checkpoint_every : (int)(avail / state_bytes) - 3;
+        nslots = spec->checkpoint_every < 0 ? -spec->checkpoint_every : (int)(avail / state_bytes) - 2;
         if (nslots > N) nslots = N;
-        if (nslots < 1 || (size_t)(nslots + 3) * state_bytes > avail)
+        if (nslots < 1 || (size_t)(nslots + 2) * state_bytes > avail)
             return bgk_internal_fail(BGK_ERR_OOM, "not enough device memory for the adjoint's checkpoints");
     }
 
@@ -970,9 +970,9 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
      * It stays in the context for the next call (freed by bgk_destroy)
      * unless it is larger than a quarter of the device memory.
      * sqrt(N): nsnap snapshots + K+1 segment states; binomial: nslots slots
-     * + 3 work states.  State i of a block at base + i * state_elems. */
+     * + 2 work states.  State i of a block at base + i * state_elems. */
     const size_t nstates_a = binomial ? (size_t)nslots : (size_t)nsnap;
-    const size_t nstates_b = binomial ? 3 : (size_t)(K + 1);
+    const size_t nstates_b = binomial ? 2 : (size_t)(K + 1);
     const size_t pi_bytes = ((size_t)NPI * pl + 2 * state_guard) * sizeof(double);
     const size_t piece[] = {nstates_a * state_bytes, nstates_b * state_bytes, pi_bytes, pi_bytes,
                             (size_t)nblk * sizeof(double), 3 * (size_t)Ny * sizeof(double),
@@ -1153,18 +1153,18 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
             for (int n = n1; n > n0; n--) ACK(rstep(state(n - 1)));
         }
     } else {
-        double *work[3] = {seg, seg + state_elems, seg + 2 * state_elems};
+        double *work[2] = {seg, seg + state_elems};
         auto slot = [&](int i) { return snaps + (size_t)i * state_elems; };
-        /* S(a + steps) from S(a) in src into dst (dst is a slot or work[2]) */
+        /* S(a + steps) from S(a) in src into dst (dst is a slot or work[1]):
+         * the intermediate states alternate between work[0] and dst itself,
+         * in the parity that ends on dst */
         auto advance = [&](const double *src, int steps, double *dst) -> cudaError_t {
             const double *cur = src;
-            int w = 0;
             for (int i = 1; i <= steps; i++) {
-                double *next = (i == steps) ? dst : work[w];
+                double *next = ((steps - i) % 2 == 0) ? dst : work[0];
                 cudaError_t e = fwd(cur, next);
                 if (e != cudaSuccess) return e;
                 cur = next;
-                w ^= 1;
             }
             return cudaSuccess;
         };
@@ -1186,8 +1186,8 @@ extern "C" int bgk_adjoint_run(bgk_ctx *c, const bgk_adjoint_spec *spec, double 
                     if (k - 1 == a) {
                         e = rstep(slot(ia));
                     } else {
-                        if ((e = advance(slot(ia), k - 1 - a, work[2])) != cudaSuccess) return e;
-                        e = rstep(work[2]);
+                        if ((e = advance(slot(ia), k - 1 - a, work[1])) != cudaSuccess) return e;
+                        e = rstep(work[1]);
                     }
                     if (e != cudaSuccess) return e;
                 }
