@@ -473,7 +473,11 @@ def main():
                                 device_id=torch.device("cuda", local))
 
     from bgk_pcm_b200 import Solver, build
-    build.build()
+    # one rank brings the in-tree library up to date; the others wait for it
+    if rank == 0:
+        build.build()
+    if dist:
+        dist.barrier()
 
     Nx, Ny = params["Nx"], params["Ny"]
     nodes = Nx * Ny
