@@ -91,9 +91,12 @@ def test_cavity2048_bit_exact_over_the_run(oracle_mod, lib):
 
 @pytest.mark.parametrize("wl_name", ["cavity4096_ra1e7", "cavity16384x4096_ra1e8"])
 def test_large_grid_slices_bit_exact(oracle_mod, lib, wl_name):
-    o, s = _run_pair(oracle_mod, wl_name, 20)
+    """20 steps, or BGK_SLICE_STEPS (longer slices are recorded that way)."""
+    steps = int(os.environ.get("BGK_SLICE_STEPS", "20"))
+    o, s = _run_pair(oracle_mod, wl_name, steps)
     try:
-        _assert_equal(o, s, f"{wl_name} after 20 steps")
+        _assert_equal(o, s, f"{wl_name} after {steps} steps")
+        print(f"{wl_name}, {steps} steps: bit-identical")
     finally:
         s.close()
         o.close()
