@@ -41,7 +41,13 @@ def _dptr(a: np.ndarray):
 
 
 class Solver:
-    """One simulation on one B200 (STEP_7/setup.f90 allocates, this creates)."""
+    """One simulation on one B200 (STEP_7/setup.f90 allocates, this creates).
+
+    precision: "f64" (the reference's), "f32", "f16" or "f32x" deviation
+    storage; tanh: "portable" (bit-identical to the CPU oracle) or "device";
+    fma: multiply-add contraction in FP64; smooth: the REAL(4) collision
+    temporaries kept in double (the form the adjoint differentiates); heat:
+    the heated wall (see heat_bits)."""
 
     def __init__(self, params, precision: str = "f64", tanh: str = "portable", fma: bool = False,
                  device: int = -1, smooth: bool = False, heat="west"):
