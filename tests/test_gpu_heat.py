@@ -162,10 +162,11 @@ def test_heat_option_refusals(lib):
     b.close()
 
 
-def test_host_program_heat_right_matches_oracle_program(tmp_path, oracle_mod, lib):
-    """bgk_thermal --heat right against the oracle's program built with the
-    FROMRIGHT branches: the same output files, bit for bit (field_check's
-    means to 1e-7, as for the west-heated program)."""
+@pytest.mark.parametrize("flag,bits", [("right", RIGHT), ("bottom", BOTTOM), ("right+bottom", RIGHT | BOTTOM)])
+def test_host_program_heat_matches_oracle_program(tmp_path, oracle_mod, lib, flag, bits):
+    """bgk_thermal --heat against the oracle's program built with the
+    FROMRIGHT / FROMBOTTOM branches: the same output files, bit for bit
+    (field_check's means to 1e-7, as for the west-heated program)."""
     from bgk_pcm_b200 import build, inputs
     from test_gpu_host import numbers
     build.build()
@@ -177,11 +178,11 @@ def test_host_program_heat_right_matches_oracle_program(tmp_path, oracle_mod, li
         d.mkdir()
         inputs.write(d / "input.dat", p)
         dirs[who] = d
-    oracle_mod.run_main(dirs["oracle"], threads=4, tanh_mode=1, heat=RIGHT)
-    r = subprocess.run([str(ROOT / "bgk_pcm_b200" / "bgk_thermal"), str(dirs["gpu"]), "--heat", "right"],
+    oracle_mod.run_main(dirs["oracle"], threads=4, tanh_mode=1, heat=bits)
+    r = subprocess.run([str(ROOT / "bgk_pcm_b200" / "bgk_thermal"), str(dirs["gpu"]), "--heat", flag],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
-    assert "Heating from right" in r.stdout
+    assert ("Heating from right" if bits & RIGHT else "Heating from left") in r.stdout
     for name in ["fort.666", "fort.667", "fort.668", "non-dim_bulk_numbers.dat", "Output_00002000.vtk"]:
         np.testing.assert_array_equal(numbers(dirs["gpu"] / name), numbers(dirs["oracle"] / name), err_msg=name)
     np.testing.assert_allclose(numbers(dirs["gpu"] / "fort.64"), numbers(dirs["oracle"] / "fort.64"), rtol=1e-7)
