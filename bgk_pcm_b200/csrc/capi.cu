@@ -664,7 +664,15 @@ int bgk_step(bgk_ctx *c, int nsteps)
     /* Launch-bound grids: the plain steps before the last two as replays of
      * a captured graph (the kernels and their order are those of the loop
      * below, so the results are the same bit for bit) */
-    if (c->graph_on && !c->graph_failed && !c->tune_flow && nsteps - 2 - t >= GRAPH_STEPS + 1) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(c->stream, &cap) != cudaSuccess) {
+        (void)cudaGetLastError();
+        cap = cudaStreamCaptureStatusActive;
+    }
+    /* (a caller capturing the context's stream into a graph of its own gets
+     * the direct launches) */
+    if (c->graph_on && !c->graph_failed && !c->tune_flow && cap == cudaStreamCaptureStatusNone &&
+        nsteps - 2 - t >= GRAPH_STEPS + 1) {
         if (!c->step_graph[c->cur ^ 1] || !c->step_graph[c->cur]) {
             /* one step launched directly first sets every kernel's attributes */
             CK(launch_plain_step(c, exact), "fused step");
